@@ -1,0 +1,252 @@
+/*
+ * supertrack_b200 — C ABI of the B200-native VoxelConstrainedSphere superimposition path.
+ *
+ * The reference (JDecunha/SuperTrack) has no C ABI: its C++ run loop calls CUDA directly. Every
+ * entry point below states which reference interface it replaces (file:line in the reference
+ * tree). Conventions:
+ *   - every function returns st_status (ST_OK == 0) and never aborts or throws;
+ *   - plain pointers and sizes only; "device" pointers are CUDA device addresses on the
+ *     context's device, everything else is host memory;
+ *   - a context is used by one host thread at a time.
+ */
+#ifndef SUPERTRACK_B200_H
+#define SUPERTRACK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ST_API __attribute__((visibility("default")))
+
+typedef enum {
+  ST_OK = 0,
+  ST_ERR_INVALID_ARGUMENT = 1,
+  ST_ERR_BAD_GEOMETRY = 2,     /* sphere diameter <= 0, non-finite input, lattice too large */
+  ST_ERR_BAD_HISTOGRAM = 3,    /* unknown type, nbins < 1, edges not finite/increasing      */
+  ST_ERR_CUDA = 4,             /* a CUDA call failed; st_ctx_last_error has the text         */
+  ST_ERR_OUT_OF_MEMORY = 5,
+  ST_ERR_CAPACITY = 6,         /* a caller buffer or a fixed capacity is too small           */
+  ST_ERR_NONFINITE_EDEP = 7,   /* a job's edep/((2/3)d) is NaN or infinite                   */
+  ST_ERR_DEVICE_OVERFLOW = 8,  /* a device-side table or export buffer overflowed            */
+  ST_ERR_NOT_FOUND = 9,
+  ST_ERR_STATE = 10,           /* call out of order (e.g. reading stats before st_run)       */
+  ST_ERR_IO = 11,
+  ST_ERR_CONFIG = 12,          /* unusable .ini macro                                        */
+  ST_ERR_NO_DEVICE = 13
+} st_status;
+
+typedef enum { ST_ZSHIFT_PLUS = 0, ST_ZSHIFT_MINUS = 1, ST_ZSHIFT_NONE = 2 } st_zshift_mode;
+typedef enum { ST_HIST_LIN = 0, ST_HIST_LOG = 1 } st_hist_type;
+typedef enum { ST_RUN_BATCHED = 0, ST_RUN_PLAIN = 1 } st_run_mode;
+
+/* Fitted lattice; same fields as SphericalGeometry (SphericalGeometry.cuh:8-23). */
+typedef struct {
+  double scoring_region_length;
+  double scoring_region_half_length;
+  double greatest_sphere_offset;
+  int32_t num_spheres_linear;
+  int32_t reserved;
+  double sphere_diameter;
+  double sphere_radius;
+} st_geometry;
+
+/* One track: float64 SoA deposits (x, y, z in nm; edep in eV). on_device != 0 means the four
+ * pointers are device addresses that stay valid and unchanged until st_jobs_clear; otherwise
+ * they are host memory (pinned memory makes the copy asynchronous) read during st_run. The
+ * track is never modified. */
+typedef struct {
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* edep;
+  int64_t n;
+  int32_t on_device;
+  int32_t reserved;
+} st_track_view;
+
+/* One superimposition job: a track, its geometry, its oversamples and the histogram it feeds. */
+typedef struct {
+  double half_length;        /* [VoxelConstrainedSphere] ScoringRegionHalfLength (nm)      */
+  double sphere_diameter;    /* [VoxelConstrainedSphere] ScoringSphereDiameter (nm)        */
+  int32_t zshift;            /* st_zshift_mode: z-origin shift +HL', -HL' or none          */
+  int32_t shift_track;       /* [VoxelConstrainedSphere] ShiftTrack                        */
+  uint32_t n_oversamples;    /* [Run] Oversamples                                          */
+  int32_t hist_id;           /* from st_hist_create                                        */
+  uint64_t seed;             /* task seed (ThreadAllocation.cc:28-31)                      */
+  uint64_t track_id;         /* second Philox key word; 0 for tasks seeded per track       */
+} st_job_desc;
+
+typedef struct {
+  uint64_t hits;             /* in-sphere deposits over all oversamples                    */
+  uint64_t spheres;          /* (oversample, sphere) pairs with at least one hit           */
+  uint64_t binned;           /* of those, the ones inside the histogram range              */
+  uint64_t inbox;            /* deposit*oversamples inside the voxel after the shift       */
+  int32_t grid_exponent;     /* exponent E0 of the job's exact accumulation grid           */
+  int32_t status;            /* st_status of this job                                      */
+} st_job_stats;
+
+/* One exported sphere of one oversample (the reference's reduced VolumeEdepPair entry,
+ * Histogram.cu:153): key = ix + iy*N + iz*N*N and its lineal energy y in keV/um. */
+typedef struct {
+  uint64_t key;
+  double y;
+  int32_t os;
+  int32_t job;
+} st_sphere;
+
+typedef struct st_ctx st_ctx;
+
+ST_API const char* st_status_string(st_status s);
+ST_API const char* st_version(void);
+
+/* --- host-only helpers (no GPU needed) ------------------------------------------------------ */
+
+/* SphericalGeometry(half_length, sphere_diameter) — SphericalGeometry.cu:7-32. */
+ST_API st_status st_geometry_make(double half_length, double sphere_diameter, st_geometry* out);
+
+/* utils::LinSpace / utils::LogSpace as used by Histogram::ConstructBins —
+ * utils.cc:8-31, Histogram.cu:53-72. edges_out holds nbins+1 doubles. */
+ST_API st_status st_hist_edges(int32_t type, int32_t nbins, float lower, float upper,
+                               double* edges_out);
+
+/* The Philox4x32-10 block function used for the oversample shifts. */
+ST_API st_status st_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* (sx, sy) of oversamples os_begin .. os_begin+n_os-1, interleaved in sxsy[2*n_os]: the shift
+ * the fused kernel applies (replaces the cuRAND draw of GenerateRandomXYShift,
+ * VoxelConstrainedSphereMethod.cu:61-83, and the shift formula at :176-177). */
+ST_API st_status st_oversample_shifts(const st_geometry* g, int32_t shift_track, uint64_t seed,
+                                      uint64_t track_id, uint32_t os_begin, uint32_t n_os,
+                                      double* sxsy);
+
+/* Fixed-point helpers of the exact per-sphere accumulation (exposed for verification). */
+ST_API int32_t st_grid_exponent(int32_t e_min, int32_t e_max, int64_t n, int32_t any_nonzero);
+ST_API void st_to_fixed(double v, int32_t e0, uint64_t* lo, uint64_t* hi);
+ST_API double st_from_fixed(uint64_t lo, uint64_t hi, int32_t e0);
+
+/* --- context ---------------------------------------------------------------------------- */
+
+/* Creates a context on `device`; stream NULL creates a private non-blocking stream, otherwise
+ * all work is enqueued on the given cudaStream_t. Replaces the per-worker CUDA state of
+ * SuperTrackManager::Run's forked processes (SuperTrackManager.cu:53-56). */
+ST_API st_status st_ctx_create(int32_t device, void* stream, st_ctx** out);
+ST_API st_status st_ctx_destroy(st_ctx* ctx);
+ST_API st_status st_ctx_set_stream(st_ctx* ctx, void* stream);
+ST_API st_status st_ctx_last_error(const st_ctx* ctx, char* buf, size_t len);
+ST_API int32_t st_ctx_sm_count(const st_ctx* ctx);
+/* Enables CUDA-event timing of the prepare and fused kernels inside st_run. */
+ST_API st_status st_ctx_enable_timing(st_ctx* ctx, int32_t on);
+/* Milliseconds of the last st_run: prepare kernel, fused kernel, and number of kernel launches. */
+ST_API st_status st_ctx_last_timing(const st_ctx* ctx, float* prepare_ms, float* fused_ms,
+                                    int32_t* launches);
+/* Measured FP64 add/multiply issue rate of the device (operations per second). */
+ST_API st_status st_measure_fp64_peak(st_ctx* ctx, double* ops_per_second);
+/* Tuning knobs: target deposit*oversamples per work item, resident CTAs (0 = one per SM). */
+ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid);
+
+/* --- histograms (device accumulators) ------------------------------------------------------ */
+
+/* Histogram(nbins, binLower, binUpper, type) — Histogram.cu:16-28 / :30-43. */
+ST_API st_status st_hist_create(st_ctx* ctx, int32_t type, int32_t nbins, float lower,
+                                float upper, int32_t* hist_id);
+/* Copies the accumulated f(y) counts (int64) and y*f(y) sums (float64) to host arrays of nbins
+ * (either may be NULL). Replaces Histogram::AccumulateCPUHistogram/GetCPUHistogram
+ * (Histogram.cu:177-186, Histogram.cuh:47). */
+ST_API st_status st_hist_read(st_ctx* ctx, int32_t hist_id, int64_t* counts, double* yfy);
+/* Zeroes one histogram, or all of them with hist_id = -1. */
+ST_API st_status st_hist_reset(st_ctx* ctx, int32_t hist_id);
+/* Copies every histogram of the context in two transfers: counts/yfy receive all bins in
+ * histogram creation order (st_hist_offset gives each histogram's first bin); cap is the room
+ * in each array; n_bins receives the total. */
+ST_API st_status st_hist_read_all(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap,
+                                  int64_t* n_bins);
+ST_API st_status st_hist_offset(const st_ctx* ctx, int32_t hist_id, int64_t* first_bin);
+ST_API st_status st_hist_nbins(const st_ctx* ctx, int32_t hist_id, int32_t* nbins);
+ST_API st_status st_hist_edges_of(const st_ctx* ctx, int32_t hist_id, double* edges);
+
+/* --- jobs ---------------------------------------------------------------------------------- */
+
+/* Queues one track for superimposition. Replaces, per task, Track::AllocateAndLoadTrack +
+ * VoxelConstrainedSphereMethod::AllocateTrackProcess + the N_os calls of ProcessTrack and
+ * Histogram::SortReduceAndAddToHistogram (SuperTrackManager.cu:61-75). */
+ST_API st_status st_job_submit(st_ctx* ctx, const st_track_view* track, const st_job_desc* desc,
+                               int32_t* job_id);
+/* Runs every queued job that has not run yet. ST_RUN_BATCHED: one prepare launch and one
+ * persistent work-stealing launch for all of them; ST_RUN_PLAIN: one track at a time, each
+ * with its own launches and a host synchronisation (the reference's per-task loop shape). */
+ST_API st_status st_run(st_ctx* ctx, int32_t mode);
+ST_API st_status st_job_stats_get(st_ctx* ctx, int32_t job_id, st_job_stats* out);
+/* Queues n jobs at once (tracks[i] with descs[i]); job_ids may be NULL. */
+ST_API st_status st_job_submit_many(st_ctx* ctx, int32_t n, const st_track_view* tracks,
+                                    const st_job_desc* descs, int32_t* job_ids);
+/* Marks every queued job as not yet run, so the next st_run runs the same jobs again (host
+ * tracks are copied again; the launch set-up of an unchanged batch is reused). */
+ST_API st_status st_jobs_reset(st_ctx* ctx);
+/* Forgets all jobs (their device copies are released for reuse). */
+ST_API st_status st_jobs_clear(st_ctx* ctx);
+ST_API st_status st_jobs_count(const st_ctx* ctx, int32_t* n);
+
+/* Like st_run(ST_RUN_BATCHED) but also returns every (oversample, sphere) with its lineal
+ * energy, in no particular order; spheres_out has room for cap records. The exported list is
+ * the reference's per-oversample reduced VolumeEdepPair (Histogram.cu:150-153). */
+ST_API st_status st_run_export(st_ctx* ctx, st_sphere* spheres_out, int64_t cap, int64_t* n_out);
+
+/* --- macro-level run (SuperTrackManager) ----------------------------------------------------- */
+
+typedef struct {
+  int64_t n_tracks;          /* "Number of Tracks"                                        */
+  int64_t n_oversamples;     /* "Number of Oversamples"                                   */
+  int64_t n_effective;       /* "Effective Number of Tracks"                              */
+  int64_t random_seed;       /* [Run] RandomSeed after the time(NULL) default             */
+  int64_t deposits;          /* deposits over all tracks                                  */
+  int32_t nbins;
+  int32_t reserved;
+} st_run_info;
+
+/* SuperTrackManager::Initialize(new INIReader(path)) + Run() (SuperTrackManager.cu:28-102):
+ * reads the macro, enumerates the track folder, derives the task seeds, runs every task on
+ * the GPU and writes <[Output] Path><NamePrefix><seed>.csv/.json unless write_output == 0.
+ * counts/yfy receive the summed spectrum (nbins_cap entries available). */
+ST_API st_status st_run_macro(const char* ini_path, int32_t device, int32_t write_output,
+                              int64_t* counts, double* yfy, int32_t nbins_cap,
+                              st_run_info* info, char* err, size_t err_len);
+
+/* Writes a track file (the format SuperTrackManager's folder loop reads). */
+ST_API st_status st_track_file_write(const char* path, uint64_t n_tracks, const uint64_t* index,
+                                     uint64_t n_deposits, const double* x, const double* y,
+                                     const double* z, const double* edep);
+
+/* --- .ini access (INIReader, extern/inih/INIReader.h) --------------------------------------- */
+typedef struct st_ini st_ini;
+ST_API st_status st_ini_open(const char* path, st_ini** out, int32_t* parse_error);
+ST_API st_status st_ini_from_string(const char* text, st_ini** out, int32_t* parse_error);
+ST_API void st_ini_close(st_ini* ini);
+ST_API st_status st_ini_get(const st_ini* ini, const char* section, const char* name,
+                            const char* default_value, char* buf, size_t len);
+ST_API long st_ini_get_integer(const st_ini* ini, const char* section, const char* name, long dflt);
+ST_API double st_ini_get_real(const st_ini* ini, const char* section, const char* name, double dflt);
+ST_API float st_ini_get_float(const st_ini* ini, const char* section, const char* name, float dflt);
+ST_API int32_t st_ini_get_boolean(const st_ini* ini, const char* section, const char* name,
+                                  int32_t dflt);
+
+/* Task list of a macro: ThreadAllocator::ReturnThreadAllocations (ThreadAllocator.cc:51-109)
+ * flattened; per task: thread id, entry/exit points, task seed, file ordinal (1-based). */
+typedef struct {
+  int64_t entry;
+  int64_t exit;
+  int64_t seed;
+  int32_t thread_id;
+  int32_t file_ordinal;
+  int32_t n_oversamples;
+  int32_t track_in_file;
+} st_task;
+ST_API st_status st_macro_tasks(const char* ini_path, st_task* tasks, int64_t cap, int64_t* n_out,
+                                char* err, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SUPERTRACK_B200_H */

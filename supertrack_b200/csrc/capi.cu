@@ -1,0 +1,811 @@
+// Host runtime behind the C ABI (include/supertrack_b200.h): contexts, device arenas,
+// histograms, job queues and the launches of the prepare and fused kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/supertrack_b200.h"
+#include "host_model.h"
+#include "st_device.cuh"
+
+namespace st {
+cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, cudaStream_t s);
+cudaError_t configure_fused(int smem_hist_bins);
+cudaError_t launch_fused(const FusedParams& p, int grid, cudaStream_t s);
+cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
+}  // namespace st
+
+namespace {
+
+using st::HistDev;
+using st::JobAux;
+using st::JobDev;
+using st::WorkItem;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) { b.p = nullptr; return e; }
+  b.bytes = bytes;
+  return cudaSuccess;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+struct HistHost {
+  int32_t type = 0, nbins = 0;
+  float lower = 0, upper = 0;
+  std::vector<double> edges;
+  int64_t off = 0;        // first bin in the context's count/yfy arenas
+  int64_t eoff = 0;       // first edge in the context's edge arena
+};
+
+struct JobHost {
+  st_track_view track{};
+  st_job_desc desc{};
+  st::Geometry g{};
+  int64_t n_pad = 0;
+  int64_t prep_off = 0;
+  int64_t arena_off = -1;  // host tracks: offset of the device copy inside the track arena
+  bool ran = false;
+  st_job_stats stats{};
+};
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+uint32_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return (uint32_t)std::min<uint64_t>(p, 1ull << 31);
+}
+
+}  // namespace
+
+struct st_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  std::string err;
+  std::vector<HistHost> hists;
+  std::vector<JobHost> jobs;
+
+  DevBuf track_arena;
+  DevBuf px, py, pdz2, pv, pkz;
+  DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err;
+  DevBuf g_keys, g_lo, g_hi, g_used, g_count;
+  uint32_t gcap = 0;
+  int ggrid = 0;
+  bool g_dirty = false;
+  DevBuf ex_buf, ex_count;
+  // all histograms live in three arenas so that every spectrum can be read in two copies
+  DevBuf h_counts, h_yfy, h_edges;
+  int64_t h_bins = 0, h_edge_total = 0;
+
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float t_prep = 0, t_fused = 0;
+  int32_t launches = 0;
+
+  int64_t item_cost = 1 << 20;
+  int grid_override = 0;
+  int smem_hist_bins = 4096;
+  bool fused_configured = false;
+
+  // launch set-up of the last batched range, reused when the same jobs run again
+  bool cache_valid = false;
+  size_t cache_first = 0, cache_last = 0;
+  std::vector<JobAux> cache_aux;
+  st::PrepareParams cache_pp{};
+  st::FusedParams cache_fp{};
+  int64_t cache_blocks = 0;
+  int cache_grid = 0;
+  int64_t cache_arena_total = 0;
+};
+
+namespace {
+
+st_status cuda_fail(st_ctx* c, cudaError_t e, const char* what) {
+  c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? ST_ERR_OUT_OF_MEMORY : ST_ERR_CUDA;
+}
+
+#define ST_CUDA(call, what)                              \
+  do {                                                   \
+    cudaError_t e__ = (call);                            \
+    if (e__ != cudaSuccess) return cuda_fail(c, e__, what); \
+  } while (0)
+
+st_status init_spill_tables(st_ctx* c, uint32_t gcap, int grid) {
+  const size_t slots = (size_t)gcap * (size_t)grid;
+  ST_CUDA(ensure(c->g_keys, slots * 8), "spill table keys");
+  ST_CUDA(ensure(c->g_lo, slots * 8), "spill table lo");
+  ST_CUDA(ensure(c->g_hi, slots * 8), "spill table hi");
+  ST_CUDA(ensure(c->g_used, slots * 4), "spill table used list");
+  ST_CUDA(ensure(c->g_count, (size_t)grid * 4), "spill table counters");
+  ST_CUDA(cudaMemsetAsync(c->g_keys.p, 0xFF, slots * 8, c->stream), "spill init");
+  ST_CUDA(cudaMemsetAsync(c->g_lo.p, 0, slots * 8, c->stream), "spill init");
+  ST_CUDA(cudaMemsetAsync(c->g_hi.p, 0, slots * 8, c->stream), "spill init");
+  ST_CUDA(cudaMemsetAsync(c->g_count.p, 0, (size_t)grid * 4, c->stream), "spill init");
+  c->gcap = gcap;
+  c->ggrid = grid;
+  c->g_dirty = false;
+  return ST_OK;
+}
+
+// Copies the host-resident tracks of jobs [first, last) into the track arena; adjacent host
+// ranges are merged into one copy per coordinate array.
+st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena_total) {
+  double* arena = (double*)c->track_arena.p;
+  size_t j = first;
+  while (j < last) {
+    JobHost& J = c->jobs[j];
+    if (J.track.on_device || J.track.n == 0) { ++j; continue; }
+    size_t k = j + 1;
+    int64_t n = J.track.n;
+    while (k < last) {
+      const JobHost& K = c->jobs[k];
+      if (K.track.on_device || K.track.n == 0 || K.arena_off != J.arena_off + n ||
+          K.track.x != J.track.x + n || K.track.y != J.track.y + n ||
+          K.track.z != J.track.z + n || K.track.edep != J.track.edep + n)
+        break;
+      n += K.track.n;
+      ++k;
+    }
+    const double* src[4] = {J.track.x, J.track.y, J.track.z, J.track.edep};
+    for (int a = 0; a < 4; ++a)
+      ST_CUDA(cudaMemcpyAsync(arena + (size_t)arena_total * a + J.arena_off, src[a],
+                              (size_t)n * 8, cudaMemcpyHostToDevice, c->stream),
+              "track upload");
+    j = k;
+  }
+  return ST_OK;
+}
+
+// Builds the device tables (jobs, aux, histograms, work items, prepare blocks) of jobs
+// [first, last) and the launch parameters; stores them in the context cache.
+st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
+  const size_t nj = last - first;
+  int64_t prep_total = 0, arena_total = 0, max_pad = 0;
+  for (size_t j = first; j < last; ++j) {
+    JobHost& J = c->jobs[j];
+    J.n_pad = round_up(std::max<int64_t>(J.track.n, 1), st::kWarpTile);
+    J.prep_off = prep_total;
+    prep_total += J.n_pad;
+    max_pad = std::max(max_pad, J.n_pad);
+    J.arena_off = -1;
+    if (!J.track.on_device && J.track.n > 0) {
+      J.arena_off = arena_total;
+      arena_total += J.track.n;
+    }
+  }
+  ST_CUDA(ensure(c->px, prep_total * 8), "prepared arena");
+  ST_CUDA(ensure(c->py, prep_total * 8), "prepared arena");
+  ST_CUDA(ensure(c->pdz2, prep_total * 8), "prepared arena");
+  ST_CUDA(ensure(c->pv, prep_total * 8), "prepared arena");
+  ST_CUDA(ensure(c->pkz, prep_total * 4), "prepared arena");
+  ST_CUDA(ensure(c->track_arena, (size_t)arena_total * 32), "track arena");
+  double* arena = (double*)c->track_arena.p;
+
+  std::vector<JobDev> jd(nj);
+  std::vector<JobAux> aux(nj);
+  std::vector<int64_t> blk(nj + 1, 0);
+  for (size_t i = 0; i < nj; ++i) {
+    JobHost& J = c->jobs[first + i];
+    JobDev& D = jd[i];
+    if (J.track.on_device) {
+      D.x = J.track.x; D.y = J.track.y; D.z = J.track.z; D.edep = J.track.edep;
+    } else {
+      D.x = arena + J.arena_off;
+      D.y = arena + (size_t)arena_total + J.arena_off;
+      D.z = arena + (size_t)arena_total * 2 + J.arena_off;
+      D.edep = arena + (size_t)arena_total * 3 + J.arena_off;
+    }
+    D.n = J.track.n;
+    D.n_pad = J.n_pad;
+    D.prep_off = J.prep_off;
+    D.HL = J.g.scoringRegionHalfLength;
+    D.L = J.g.scoringRegionLength;
+    D.gSO = J.g.greatestSphereOffset;
+    D.d = J.g.sphereDiameter;
+    D.inv_d = 1.0 / J.g.sphereDiameter;
+    D.r2 = J.g.sphereRadius * J.g.sphereRadius;
+    D.denom = (2. / 3.) * J.g.sphereDiameter;
+    D.zsh = J.desc.zshift == ST_ZSHIFT_PLUS ? J.g.scoringRegionHalfLength
+          : J.desc.zshift == ST_ZSHIFT_MINUS ? -J.g.scoringRegionHalfLength : 0.0;
+    D.N = (uint32_t)J.g.numSpheresLinear;
+    D.N2 = (uint64_t)D.N * (uint64_t)D.N;
+    D.seed = J.desc.seed;
+    D.track_id = J.desc.track_id;
+    D.n_os = (int32_t)J.desc.n_oversamples;
+    D.shift_track = J.desc.shift_track ? 1 : 0;
+    D.hist = J.desc.hist_id;
+    JobAux& A = aux[i];
+    std::memset(&A, 0, sizeof(A));
+    A.e_min = 0x7fffffff;
+    A.e_max = (int32_t)0x80000000;
+    blk[i + 1] = blk[i] + (J.n_pad + st::kPrepSlotsPerBlock - 1) / st::kPrepSlotsPerBlock;
+  }
+  std::vector<HistDev> hd(c->hists.size());
+  for (size_t h = 0; h < c->hists.size(); ++h) {
+    hd[h].edges = (const double*)c->h_edges.p + c->hists[h].eoff;
+    hd[h].counts = (unsigned long long*)c->h_counts.p + c->hists[h].off;
+    hd[h].yfy = (double*)c->h_yfy.p + c->hists[h].off;
+    hd[h].nbins = c->hists[h].nbins;
+  }
+
+  // work items: oversample blocks of roughly item_cost deposit*oversamples, longest first
+  std::vector<WorkItem> items;
+  for (size_t i = 0; i < nj; ++i) {
+    const JobHost& J = c->jobs[first + i];
+    const int64_t nos = J.desc.n_oversamples;
+    if (nos == 0 || J.track.n == 0) continue;
+    int64_t blk_os = std::max<int64_t>(1, c->item_cost / J.n_pad);
+    blk_os = std::min<int64_t>(blk_os, nos);
+    for (int64_t o = 0; o < nos; o += blk_os) {
+      WorkItem w;
+      w.job = (int32_t)i;
+      w.os_begin = (int32_t)o;
+      w.os_count = (int32_t)std::min<int64_t>(blk_os, nos - o);
+      w.pad = 0;
+      items.push_back(w);
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
+    return jd[a.job].n_pad * a.os_count > jd[b.job].n_pad * b.os_count;
+  });
+
+  ST_CUDA(ensure(c->d_jobs, nj * sizeof(JobDev)), "job table");
+  ST_CUDA(ensure(c->d_aux, nj * sizeof(JobAux)), "job aux");
+  ST_CUDA(ensure(c->d_hists, std::max<size_t>(1, hd.size()) * sizeof(HistDev)), "hist table");
+  ST_CUDA(ensure(c->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)), "items");
+  ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
+  ST_CUDA(ensure(c->d_counter, 16), "work counter");
+  ST_CUDA(ensure(c->d_err, 16), "error flags");
+  ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, jd.data(), nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
+  if (!hd.empty())
+    ST_CUDA(cudaMemcpyAsync(c->d_hists.p, hd.data(), hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
+  if (!items.empty())
+    ST_CUDA(cudaMemcpyAsync(c->d_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, c->stream), "upload items");
+  ST_CUDA(cudaMemcpyAsync(c->d_blk.p, blk.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
+
+  // spill tables
+  int grid = c->grid_override > 0 ? c->grid_override : c->sm_count;
+  grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)items.size()));
+  const uint32_t gcap = next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024));
+  if (gcap > c->gcap || grid > c->ggrid || c->g_dirty) {
+    st_status s = init_spill_tables(c, std::max(gcap, c->gcap), std::max(grid, c->ggrid));
+    if (s != ST_OK) return s;
+  }
+  if (!c->fused_configured) {
+    ST_CUDA(st::configure_fused(c->smem_hist_bins), "configure fused kernel");
+    c->fused_configured = true;
+  }
+
+  st::PrepareParams& pp = c->cache_pp;
+  pp.jobs = (const JobDev*)c->d_jobs.p;
+  pp.aux = (JobAux*)c->d_aux.p;
+  pp.n_jobs = (int32_t)nj;
+  pp.blk_prefix = (const int64_t*)c->d_blk.p;
+  pp.PX = (double*)c->px.p;
+  pp.PY = (double*)c->py.p;
+  pp.PDZ2 = (double*)c->pdz2.p;
+  pp.PV = (double*)c->pv.p;
+  pp.PKZ = (uint32_t*)c->pkz.p;
+
+  st::FusedParams& fp = c->cache_fp;
+  fp.jobs = pp.jobs;
+  fp.aux = pp.aux;
+  fp.hists = (const HistDev*)c->d_hists.p;
+  fp.items = (const WorkItem*)c->d_items.p;
+  fp.n_items = (int32_t)items.size();
+  fp.flush_threshold = 1024;
+  fp.work_counter = (unsigned int*)c->d_counter.p;
+  fp.PX = pp.PX; fp.PY = pp.PY; fp.PDZ2 = pp.PDZ2; fp.PV = pp.PV; fp.PKZ = pp.PKZ;
+  fp.gkeys = (uint64_t*)c->g_keys.p;
+  fp.glo = (unsigned long long*)c->g_lo.p;
+  fp.ghi = (unsigned long long*)c->g_hi.p;
+  fp.gused = (uint32_t*)c->g_used.p;
+  fp.gcount = (unsigned int*)c->g_count.p;
+  fp.gcap = c->gcap;
+  fp.smem_hist_bins = c->smem_hist_bins;
+  fp.export_buf = nullptr;
+  fp.export_count = nullptr;
+  fp.export_cap = 0;
+  fp.error_flags = (int*)c->d_err.p;
+
+  c->cache_aux = std::move(aux);
+  c->cache_blocks = blk[nj];
+  c->cache_grid = items.empty() ? 0 : grid;
+  c->cache_arena_total = arena_total;
+  c->cache_first = first;
+  c->cache_last = last;
+  c->cache_valid = !want_export;
+  return ST_OK;
+}
+
+// Runs jobs [first, last) of the context in one prepare launch and one fused launch.
+st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int64_t ex_cap,
+                    int64_t* ex_n) {
+  if (first >= last) {
+    if (ex_n) *ex_n = 0;
+    return ST_OK;
+  }
+  const size_t nj = last - first;
+  const bool reuse = !ex_out && c->cache_valid && c->cache_first == first && c->cache_last == last;
+  if (!reuse) {
+    st_status s = build_tables(c, first, last, ex_out != nullptr);
+    if (s != ST_OK) { c->cache_valid = false; return s; }
+  }
+  {
+    st_status s = upload_host_tracks(c, first, last, c->cache_arena_total);
+    if (s != ST_OK) return s;
+  }
+  ST_CUDA(cudaMemcpyAsync(c->d_aux.p, c->cache_aux.data(), nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
+  ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
+  ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
+
+  st::FusedParams fp = c->cache_fp;
+  if (ex_out) {
+    ST_CUDA(ensure(c->ex_buf, (size_t)std::max<int64_t>(ex_cap, 1) * sizeof(st::SphereRecord)), "export buffer");
+    ST_CUDA(ensure(c->ex_count, 16), "export counter");
+    ST_CUDA(cudaMemsetAsync(c->ex_count.p, 0, 16, c->stream), "export counter");
+    fp.export_buf = (st::SphereRecord*)c->ex_buf.p;
+    fp.export_count = (unsigned long long*)c->ex_count.p;
+    fp.export_cap = (unsigned long long)ex_cap;
+  }
+
+  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
+  ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->stream), "prepare launch");
+  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+  ST_CUDA(st::launch_fused(fp, c->cache_grid, c->stream), "fused launch");
+  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
+  c->launches += (c->cache_blocks > 0 ? 1 : 0) + (c->cache_grid > 0 ? 1 : 0);
+
+  // ---- results
+  std::vector<JobAux> aux(nj);
+  ST_CUDA(cudaMemcpyAsync(aux.data(), c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
+  int errflags[4] = {0, 0, 0, 0};
+  ST_CUDA(cudaMemcpyAsync(errflags, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
+  unsigned long long exn = 0;
+  if (ex_out) ST_CUDA(cudaMemcpyAsync(&exn, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
+  ST_CUDA(cudaStreamSynchronize(c->stream), "run");
+  if (c->timing) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    c->t_prep += a;
+    c->t_fused += b;
+  }
+  st_status result = ST_OK;
+  for (size_t i = 0; i < nj; ++i) {
+    JobHost& J = c->jobs[first + i];
+    J.ran = true;
+    J.stats.hits = aux[i].hits;
+    J.stats.spheres = aux[i].spheres;
+    J.stats.binned = aux[i].binned;
+    J.stats.inbox = aux[i].inbox;
+    J.stats.grid_exponent = st::choose_grid_exponent(aux[i].e_min, aux[i].e_max, J.track.n,
+                                                     aux[i].flags & st::kAuxNonzero);
+    J.stats.status = (aux[i].flags & st::kAuxNonfinite) ? ST_ERR_NONFINITE_EDEP : ST_OK;
+    if (J.stats.status != ST_OK && result == ST_OK) {
+      result = ST_ERR_NONFINITE_EDEP;
+      c->err = "job " + std::to_string(first + i) + " has a non-finite edep/((2/3)d); it was skipped";
+    }
+  }
+  if (errflags[0] & 1) {
+    c->g_dirty = true;
+    c->cache_valid = false;
+    c->err = "spill table overflow";
+    return ST_ERR_DEVICE_OVERFLOW;
+  }
+  if (ex_out) {
+    if ((errflags[0] & 2) || exn > (unsigned long long)ex_cap) {
+      if (ex_n) *ex_n = (int64_t)exn;
+      c->err = "export buffer too small";
+      return ST_ERR_CAPACITY;
+    }
+    std::vector<st::SphereRecord> rec((size_t)exn);
+    if (exn) {
+      ST_CUDA(cudaMemcpy(rec.data(), c->ex_buf.p, (size_t)exn * sizeof(st::SphereRecord), cudaMemcpyDeviceToHost), "read export");
+    }
+    for (size_t i = 0; i < rec.size(); ++i) {
+      ex_out[i].key = rec[i].key;
+      ex_out[i].y = rec[i].y;
+      ex_out[i].os = rec[i].os;
+      ex_out[i].job = rec[i].job + (int32_t)first;
+    }
+    if (ex_n) *ex_n = (int64_t)exn;
+  }
+  return result;
+}
+
+}  // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+extern "C" {
+
+const char* st_status_string(st_status s) {
+  switch (s) {
+    case ST_OK: return "ok";
+    case ST_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case ST_ERR_BAD_GEOMETRY: return "bad geometry";
+    case ST_ERR_BAD_HISTOGRAM: return "bad histogram specification";
+    case ST_ERR_CUDA: return "CUDA error";
+    case ST_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case ST_ERR_CAPACITY: return "capacity exceeded";
+    case ST_ERR_NONFINITE_EDEP: return "non-finite energy deposit";
+    case ST_ERR_DEVICE_OVERFLOW: return "device table overflow";
+    case ST_ERR_NOT_FOUND: return "not found";
+    case ST_ERR_STATE: return "invalid state";
+    case ST_ERR_IO: return "I/O error";
+    case ST_ERR_CONFIG: return "configuration error";
+    case ST_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+const char* st_version(void) { return "supertrack_b200 0.1.0 (sm_100a)"; }
+
+st_status st_geometry_make(double half_length, double sphere_diameter, st_geometry* out) {
+  if (!out) return ST_ERR_INVALID_ARGUMENT;
+  st::Geometry g;
+  if (st::make_geometry(half_length, sphere_diameter, &g) != 0) return ST_ERR_BAD_GEOMETRY;
+  out->scoring_region_length = g.scoringRegionLength;
+  out->scoring_region_half_length = g.scoringRegionHalfLength;
+  out->greatest_sphere_offset = g.greatestSphereOffset;
+  out->num_spheres_linear = g.numSpheresLinear;
+  out->reserved = 0;
+  out->sphere_diameter = g.sphereDiameter;
+  out->sphere_radius = g.sphereRadius;
+  return ST_OK;
+}
+
+st_status st_hist_edges(int32_t type, int32_t nbins, float lower, float upper, double* edges_out) {
+  if (!edges_out) return ST_ERR_INVALID_ARGUMENT;
+  std::vector<double> e;
+  if (!st::MakeEdges(type, nbins, lower, upper, &e)) return ST_ERR_BAD_HISTOGRAM;
+  std::memcpy(edges_out, e.data(), e.size() * sizeof(double));
+  return ST_OK;
+}
+
+st_status st_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  if (!ctr || !key || !out) return ST_ERR_INVALID_ARGUMENT;
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  st::philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = c[i];
+  return ST_OK;
+}
+
+st_status st_oversample_shifts(const st_geometry* g, int32_t shift_track, uint64_t seed,
+                               uint64_t track_id, uint32_t os_begin, uint32_t n_os,
+                               double* sxsy) {
+  if (!g || (!sxsy && n_os)) return ST_ERR_INVALID_ARGUMENT;
+  for (uint32_t i = 0; i < n_os; ++i) {
+    float ux, uy;
+    st::shift_uniforms(seed, track_id, os_begin + i, shift_track, &ux, &uy);
+    sxsy[2 * i] = st::shift_from_uniform(ux, g->scoring_region_length, g->scoring_region_half_length);
+    sxsy[2 * i + 1] = st::shift_from_uniform(uy, g->scoring_region_length, g->scoring_region_half_length);
+  }
+  return ST_OK;
+}
+
+int32_t st_grid_exponent(int32_t e_min, int32_t e_max, int64_t n, int32_t any_nonzero) {
+  return st::choose_grid_exponent(e_min, e_max, n, any_nonzero);
+}
+
+void st_to_fixed(double v, int32_t e0, uint64_t* lo, uint64_t* hi) {
+  uint64_t a = 0, b = 0;
+  st::to_fixed(v, e0, &a, &b);
+  if (lo) *lo = a;
+  if (hi) *hi = b;
+}
+
+double st_from_fixed(uint64_t lo, uint64_t hi, int32_t e0) { return st::from_fixed(lo, hi, e0); }
+
+st_status st_ctx_create(int32_t device, void* stream, st_ctx** out) {
+  if (!out) return ST_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return ST_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return ST_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return ST_ERR_CUDA;
+  st_ctx* c = new st_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      return ST_ERR_CUDA;
+    }
+    c->own_stream = true;
+  }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+  *out = c;
+  return ST_OK;
+}
+
+st_status st_ctx_destroy(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pv, &c->pkz,
+                    &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
+                    &c->d_counter, &c->d_err, &c->g_keys, &c->g_lo, &c->g_hi,
+                    &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
+                    &c->h_yfy, &c->h_edges};
+  for (DevBuf* b : bufs) release(*b);
+  for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return ST_OK;
+}
+
+st_status st_ctx_set_stream(st_ctx* c, void* stream) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  cudaStreamSynchronize(c->stream);
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->own_stream = false;
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return ST_ERR_CUDA;
+    c->own_stream = true;
+  }
+  return ST_OK;
+}
+
+st_status st_ctx_last_error(const st_ctx* c, char* buf, size_t len) {
+  if (!c || !buf || !len) return ST_ERR_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", c->err.c_str());
+  return ST_OK;
+}
+
+int32_t st_ctx_sm_count(const st_ctx* c) { return c ? c->sm_count : 0; }
+
+st_status st_ctx_enable_timing(st_ctx* c, int32_t on) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  c->timing = on != 0;
+  return ST_OK;
+}
+
+st_status st_ctx_last_timing(const st_ctx* c, float* prepare_ms, float* fused_ms, int32_t* launches) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  if (prepare_ms) *prepare_ms = c->t_prep;
+  if (fused_ms) *fused_ms = c->t_fused;
+  if (launches) *launches = c->launches;
+  return ST_OK;
+}
+
+st_status st_ctx_set_tuning(st_ctx* c, int64_t item_cost, int32_t grid) {
+  if (!c || item_cost < 0 || grid < 0) return ST_ERR_INVALID_ARGUMENT;
+  if (item_cost > 0) c->item_cost = item_cost;
+  c->grid_override = grid;
+  return ST_OK;
+}
+
+// Grows a histogram arena to `bytes`, keeping its contents.
+static st_status grow_arena(st_ctx* c, DevBuf& b, size_t used, size_t bytes) {
+  if (b.bytes >= bytes) return ST_OK;
+  size_t cap = std::max<size_t>(bytes, b.bytes * 2);
+  void* p = nullptr;
+  ST_CUDA(cudaMalloc(&p, cap), "histogram arena");
+  if (used) ST_CUDA(cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, c->stream), "histogram arena");
+  ST_CUDA(cudaStreamSynchronize(c->stream), "histogram arena");
+  if (b.p) cudaFree(b.p);
+  b.p = p;
+  b.bytes = cap;
+  return ST_OK;
+}
+
+st_status st_hist_create(st_ctx* c, int32_t type, int32_t nbins, float lower, float upper,
+                         int32_t* hist_id) {
+  if (!c || !hist_id) return ST_ERR_INVALID_ARGUMENT;
+  HistHost h;
+  if (!st::MakeEdges(type, nbins, lower, upper, &h.edges)) return ST_ERR_BAD_HISTOGRAM;
+  h.type = type; h.nbins = nbins; h.lower = lower; h.upper = upper;
+  cudaSetDevice(c->device);
+  h.off = c->h_bins;
+  h.eoff = c->h_edge_total;
+  st_status s;
+  if ((s = grow_arena(c, c->h_counts, (size_t)c->h_bins * 8, (size_t)(c->h_bins + nbins) * 8)) != ST_OK) return s;
+  if ((s = grow_arena(c, c->h_yfy, (size_t)c->h_bins * 8, (size_t)(c->h_bins + nbins) * 8)) != ST_OK) return s;
+  if ((s = grow_arena(c, c->h_edges, (size_t)c->h_edge_total * 8, (size_t)(c->h_edge_total + nbins + 1) * 8)) != ST_OK) return s;
+  ST_CUDA(cudaMemcpyAsync((double*)c->h_edges.p + h.eoff, h.edges.data(), h.edges.size() * 8, cudaMemcpyHostToDevice, c->stream), "histogram edges");
+  ST_CUDA(cudaMemsetAsync((unsigned long long*)c->h_counts.p + h.off, 0, (size_t)nbins * 8, c->stream), "histogram counts");
+  ST_CUDA(cudaMemsetAsync((double*)c->h_yfy.p + h.off, 0, (size_t)nbins * 8, c->stream), "histogram yfy");
+  ST_CUDA(cudaStreamSynchronize(c->stream), "histogram create");
+  c->h_bins += nbins;
+  c->h_edge_total += nbins + 1;
+  c->hists.push_back(std::move(h));
+  *hist_id = (int32_t)c->hists.size() - 1;
+  c->cache_valid = false;
+  return ST_OK;
+}
+
+st_status st_hist_read(st_ctx* c, int32_t hist_id, int64_t* counts, double* yfy) {
+  if (!c || hist_id < 0 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  const HistHost& h = c->hists[hist_id];
+  if (counts) ST_CUDA(cudaMemcpyAsync(counts, (unsigned long long*)c->h_counts.p + h.off, (size_t)h.nbins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, (double*)c->h_yfy.p + h.off, (size_t)h.nbins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  ST_CUDA(cudaStreamSynchronize(c->stream), "histogram read");
+  return ST_OK;
+}
+
+st_status st_hist_read_all(st_ctx* c, int64_t* counts, double* yfy, int64_t cap, int64_t* n_bins) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  if (n_bins) *n_bins = c->h_bins;
+  if (!counts && !yfy) return ST_OK;
+  if (cap < c->h_bins) return ST_ERR_CAPACITY;
+  if (c->h_bins == 0) return ST_OK;
+  if (counts) ST_CUDA(cudaMemcpyAsync(counts, c->h_counts.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, c->h_yfy.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  ST_CUDA(cudaStreamSynchronize(c->stream), "histogram read");
+  return ST_OK;
+}
+
+st_status st_hist_offset(const st_ctx* c, int32_t hist_id, int64_t* first_bin) {
+  if (!c || !first_bin || hist_id < 0 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  *first_bin = c->hists[hist_id].off;
+  return ST_OK;
+}
+
+st_status st_hist_reset(st_ctx* c, int32_t hist_id) {
+  if (!c || hist_id < -1 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  const int64_t off = hist_id < 0 ? 0 : c->hists[hist_id].off;
+  const int64_t nb = hist_id < 0 ? c->h_bins : c->hists[hist_id].nbins;
+  if (nb == 0) return ST_OK;
+  ST_CUDA(cudaMemsetAsync((unsigned long long*)c->h_counts.p + off, 0, (size_t)nb * 8, c->stream), "histogram reset");
+  ST_CUDA(cudaMemsetAsync((double*)c->h_yfy.p + off, 0, (size_t)nb * 8, c->stream), "histogram reset");
+  return ST_OK;
+}
+
+st_status st_hist_nbins(const st_ctx* c, int32_t hist_id, int32_t* nbins) {
+  if (!c || !nbins || hist_id < 0 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  *nbins = c->hists[hist_id].nbins;
+  return ST_OK;
+}
+
+st_status st_hist_edges_of(const st_ctx* c, int32_t hist_id, double* edges) {
+  if (!c || !edges || hist_id < 0 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  const auto& e = c->hists[hist_id].edges;
+  std::memcpy(edges, e.data(), e.size() * 8);
+  return ST_OK;
+}
+
+st_status st_job_submit(st_ctx* c, const st_track_view* track, const st_job_desc* desc,
+                        int32_t* job_id) {
+  if (!c || !track || !desc) return ST_ERR_INVALID_ARGUMENT;
+  if (track->n < 0 || (track->n > 0 && (!track->x || !track->y || !track->z || !track->edep)))
+    return ST_ERR_INVALID_ARGUMENT;
+  if (track->n > (int64_t)1 << 40) return ST_ERR_CAPACITY;
+  if (desc->hist_id < 0 || desc->hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
+  if (desc->zshift < ST_ZSHIFT_PLUS || desc->zshift > ST_ZSHIFT_NONE) return ST_ERR_INVALID_ARGUMENT;
+  if (desc->n_oversamples > 0x7fffffffu) return ST_ERR_INVALID_ARGUMENT;
+  JobHost J;
+  if (st::make_geometry(desc->half_length, desc->sphere_diameter, &J.g) != 0) return ST_ERR_BAD_GEOMETRY;
+  J.track = *track;
+  J.desc = *desc;
+  c->jobs.push_back(J);
+  c->cache_valid = false;
+  if (job_id) *job_id = (int32_t)c->jobs.size() - 1;
+  return ST_OK;
+}
+
+static size_t first_unrun(const st_ctx* c) {
+  size_t f = c->jobs.size();
+  while (f > 0 && !c->jobs[f - 1].ran) --f;
+  return f;
+}
+
+st_status st_run(st_ctx* c, int32_t mode) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->t_prep = c->t_fused = 0;
+  c->launches = 0;
+  const size_t first = first_unrun(c), last = c->jobs.size();
+  if (mode == ST_RUN_BATCHED) return run_range(c, first, last, nullptr, 0, nullptr);
+  if (mode != ST_RUN_PLAIN) return ST_ERR_INVALID_ARGUMENT;
+  st_status worst = ST_OK;
+  for (size_t j = first; j < last; ++j) {
+    const st_status s = run_range(c, j, j + 1, nullptr, 0, nullptr);
+    if (s != ST_OK && s != ST_ERR_NONFINITE_EDEP) return s;
+    if (s != ST_OK) worst = s;
+  }
+  return worst;
+}
+
+st_status st_run_export(st_ctx* c, st_sphere* spheres_out, int64_t cap, int64_t* n_out) {
+  if (!c || !spheres_out || cap < 0) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  c->t_prep = c->t_fused = 0;
+  c->launches = 0;
+  return run_range(c, first_unrun(c), c->jobs.size(), spheres_out, cap, n_out);
+}
+
+st_status st_job_stats_get(st_ctx* c, int32_t job_id, st_job_stats* out) {
+  if (!c || !out || job_id < 0 || job_id >= (int32_t)c->jobs.size()) return ST_ERR_INVALID_ARGUMENT;
+  if (!c->jobs[job_id].ran) return ST_ERR_STATE;
+  *out = c->jobs[job_id].stats;
+  return ST_OK;
+}
+
+st_status st_jobs_clear(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  c->jobs.clear();
+  c->cache_valid = false;
+  return ST_OK;
+}
+
+st_status st_jobs_reset(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  for (auto& j : c->jobs) j.ran = false;
+  return ST_OK;
+}
+
+st_status st_job_submit_many(st_ctx* c, int32_t n, const st_track_view* tracks,
+                             const st_job_desc* descs, int32_t* job_ids) {
+  if (!c || n < 0 || (n && (!tracks || !descs))) return ST_ERR_INVALID_ARGUMENT;
+  for (int32_t i = 0; i < n; ++i) {
+    int32_t id = -1;
+    const st_status s = st_job_submit(c, &tracks[i], &descs[i], &id);
+    if (s != ST_OK) return s;
+    if (job_ids) job_ids[i] = id;
+  }
+  return ST_OK;
+}
+
+st_status st_measure_fp64_peak(st_ctx* c, double* ops_per_second) {
+  if (!c || !ops_per_second) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  DevBuf out;
+  ST_CUDA(ensure(out, 4096 * 8), "fp64 probe buffer");
+  const int blocks = c->sm_count * 8, iters = 4096;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
+    ST_CUDA(st::launch_fp64_probe((double*)out.p, blocks, iters, c->stream), "fp64 probe");
+    ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+    ST_CUDA(cudaEventSynchronize(c->ev[1]), "fp64 probe");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  release(out);
+  // two FP64 operations (one multiply, one add) per chain step
+  *ops_per_second = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (best * 1e-3);
+  return ST_OK;
+}
+
+st_status st_jobs_count(const st_ctx* c, int32_t* n) {
+  if (!c || !n) return ST_ERR_INVALID_ARGUMENT;
+  *n = (int32_t)c->jobs.size();
+  return ST_OK;
+}
+
+}  // extern "C"

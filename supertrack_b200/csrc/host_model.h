@@ -1,0 +1,115 @@
+// Host-side model of the reference surface for the VoxelConstrainedSphere path: the .ini
+// reader, histogram bin edges, the task/seed allocation over a track folder and the track file
+// format that replaces the ROOT "Tracks"/"Track index" trees.
+#pragma once
+#include <stdint.h>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+namespace st {
+
+// ---------------------------------------------------------------------------------------------
+// INI reader with the semantics of the inih INIReader the reference uses
+// (extern/inih/INIReader.h): case-insensitive section/name lookup (:442-448), ';' and '#'
+// full-line comments, ';' inline comments only after whitespace (:145-149), '=' or ':'
+// separators, indented continuation lines appended with "\n" (:450-460), numbers parsed with
+// strtol(...,0)/strtod/strtof and the default returned when nothing parses (:401-427), booleans
+// true/yes/on/1 and false/no/off/0 (:429-440). ParseError() is 0, the first bad line, or -1 when
+// the file cannot be opened.
+// ---------------------------------------------------------------------------------------------
+class INIReader {
+ public:
+  explicit INIReader(const std::string& filename);
+  static INIReader FromString(const std::string& text);
+  INIReader() = default;
+
+  int ParseError() const { return _error; }
+  const std::set<std::string>& Sections() const { return _sections; }
+  std::string Get(const std::string& section, const std::string& name,
+                  const std::string& default_value) const;
+  long GetInteger(const std::string& section, const std::string& name, long default_value) const;
+  double GetReal(const std::string& section, const std::string& name, double default_value) const;
+  float GetFloat(const std::string& section, const std::string& name, float default_value) const;
+  bool GetBoolean(const std::string& section, const std::string& name, bool default_value) const;
+  bool Has(const std::string& section, const std::string& name) const;
+
+ private:
+  void ParseText(const std::string& text);
+  static std::string MakeKey(const std::string& section, const std::string& name);
+  int _error = 0;
+  std::map<std::string, std::string> _values;
+  std::set<std::string> _sections;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Bin edges (utils.cc:8-31 as called from Histogram.cu:53-72). Bounds arrive as float (the
+// reference reads them with GetFloat); the linear width is a float expression; the log bounds
+// are log10 values stored as float. Returns false for an unknown type, nbins < 1, or edges that
+// are not finite and strictly increasing (for example a log histogram with a bound <= 0).
+// ---------------------------------------------------------------------------------------------
+void LinSpace(float bottom, float top, int nbins, double* bins);
+void LogSpace(float bottom, float top, int nbins, double* bins);
+bool MakeEdges(int type, int nbins, float lower, float upper, std::vector<double>* edges);
+
+// ---------------------------------------------------------------------------------------------
+// Tasks and their seeds (ThreadTask.hh:6-31, ThreadAllocation.cc:16-32, ThreadAllocator.cc).
+// ---------------------------------------------------------------------------------------------
+struct ThreadTask {
+  std::string fileName;
+  int64_t entryPoint = 0;   // first deposit of the track in the file
+  int64_t exitPoint = 0;    // one past the last deposit
+  int64_t randomSeed = 0;
+  int32_t threadID = 0;
+  int32_t nOversamples = 1;
+  int32_t trackInFile = 0;
+};
+
+struct ThreadAllocation {
+  int32_t threadID = 0;
+  int64_t randomSeed = 0;
+  int32_t nOversamples = 1;
+  std::vector<ThreadTask> tasks;
+  // The task seed is the decimal concatenation of the run seed, the thread id and the task's
+  // position in the thread (ThreadAllocation.cc:28-31). Returns false if it overflows int64.
+  bool AddTask(const ThreadTask& task);
+};
+
+struct RunConfig {
+  std::string type;
+  std::string path;
+  long firstFile = -1;
+  long lastFile = -1;
+  long threads = 1;
+  long oversamples = 1;
+  long randomSeed = -1;
+};
+
+// Reads the [Run] keys (ThreadAllocator.cc:29-49). RandomSeed -1 becomes time(NULL).
+// Returns an empty string on success or the reason the macro is unusable.
+std::string ReadRunConfig(const INIReader& reader, RunConfig* cfg);
+
+// Folder enumeration, file limits, one task per track and the contiguous split over threads
+// (ThreadAllocator.cc:51-133). Returns an empty string on success or the error text.
+std::string ReturnThreadAllocations(const RunConfig& cfg, std::vector<ThreadAllocation>* out);
+
+// ---------------------------------------------------------------------------------------------
+// Track files. One file holds several tracks as float64 SoA deposits plus the cumulative end
+// index of every track (the role of the "Tracks" tree with branches x/y/z [nm], edep [eV] and
+// the "Track index" tree, Track.cu:25-31, ThreadAllocator.cc:138-156).
+//   offset 0   : char[8]  "STRKv001"
+//   offset 8   : uint64   n_deposits
+//   offset 16  : uint64   n_tracks
+//   offset 24  : uint64   index[n_tracks]   (cumulative end entries)
+//   then       : float64  x[n], y[n], z[n], edep[n]
+// ---------------------------------------------------------------------------------------------
+constexpr const char* kTrackFileExtension = ".strk";
+bool ReadTrackIndex(const std::string& path, std::vector<uint64_t>* index, uint64_t* n_deposits);
+bool ReadTrackDeposits(const std::string& path, int64_t begin, int64_t end, double* x, double* y,
+                       double* z, double* edep);
+bool WriteTrackFile(const std::string& path, uint64_t n_tracks, const uint64_t* index,
+                    uint64_t n_deposits, const double* x, const double* y, const double* z,
+                    const double* edep);
+
+}  // namespace st

@@ -1,0 +1,132 @@
+// Device-side data layout shared by the kernels (vcs_kernels.cu) and the host runtime (capi.cu).
+//
+// HBM layout of one batch:
+//   * input tracks: SoA float64 x, y, z, edep per job (caller memory or the context's arena);
+//   * prepared arena (written once per job, read once per oversample): for every job a padded
+//     run of warp tiles of kWarpTile deposits, stored tile by tile in "lane-blocked" order so a
+//     warp-wide load of row p reads 32 consecutive doubles while lane l owns the kDepPerLane
+//     consecutive deposits l*kDepPerLane .. l*kDepPerLane+kDepPerLane-1 of the tile:
+//       PX, PY  : x, y as loaded (padding slots hold NaN so the box test rejects them)
+//       PDZ2    : (k_z*d - a_z)^2, +inf when the deposit is outside the box in z
+//       PV      : edep / ((2/3) d)
+//       PKZ     : k_z (uint32)
+//   * spill tables: one open-addressing table per resident CTA for spheres that do not fit
+//     the CTA's shared-memory table (keys, 128-bit accumulators, used-slot list);
+//   * histograms: int64 counts and float64 y*f(y) sums per bin, one set per histogram.
+#pragma once
+#include <stdint.h>
+#include "st_core.cuh"
+
+namespace st {
+
+constexpr int kDepPerLane = 8;                  // deposits owned by one lane inside a warp tile
+constexpr int kWarpTile = 32 * kDepPerLane;     // deposits per warp tile
+constexpr uint64_t kEmptyKey = ~0ull;           // never a valid sphere key (keys < 2^63)
+
+struct JobDev {
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* edep;
+  int64_t n;          // deposits in the track
+  int64_t n_pad;      // n rounded up to a whole number of warp tiles
+  int64_t prep_off;   // first slot of this job in the prepared arena
+  double HL;          // scoringRegionHalfLength (after lattice fitting)
+  double L;           // scoringRegionLength
+  double gSO;         // greatestSphereOffset
+  double d;           // sphere diameter
+  double inv_d;       // RN(1/d), used by the fast lattice-index path
+  double r2;          // RN(r*r)
+  double denom;       // RN(RN(2/3)*d): lineal-energy denominator
+  double zsh;         // z-origin shift added to every z
+  uint64_t N2;        // N*N
+  uint64_t seed;
+  uint64_t track_id;
+  uint32_t N;
+  int32_t n_os;
+  int32_t shift_track;
+  int32_t hist;       // histogram index
+};
+
+// Per-job values produced on the device.
+struct JobAux {
+  int32_t e_min;          // min ulp exponent over nonzero contributions
+  int32_t e_max;          // max ulp exponent over nonzero contributions
+  int32_t flags;          // kAuxNonzero | kAuxNonfinite
+  int32_t pad;
+  unsigned long long hits;     // in-sphere deposits summed over all oversamples
+  unsigned long long spheres;  // (oversample, sphere) pairs with at least one hit
+  unsigned long long binned;   // of those, the ones that landed inside the histogram range
+  unsigned long long inbox;    // deposit*oversamples inside the voxel after the shift
+};
+constexpr int kAuxNonzero = 1;
+constexpr int kAuxNonfinite = 2;
+
+struct HistDev {
+  const double* edges;            // nbins + 1 edges
+  unsigned long long* counts;     // nbins
+  double* yfy;                    // nbins
+  int32_t nbins;
+  int32_t pad;
+};
+
+// One unit of work for the persistent kernel: a contiguous block of oversamples of one job.
+struct WorkItem {
+  int32_t job;
+  int32_t os_begin;
+  int32_t os_count;
+  int32_t pad;
+};
+
+// One exported sphere: (oversample, key, lineal energy, hit deposits).
+struct SphereRecord {
+  uint64_t key;
+  double y;
+  int32_t os;
+  int32_t job;
+};
+
+struct FusedParams {
+  const JobDev* jobs;
+  JobAux* aux;
+  const HistDev* hists;
+  const WorkItem* items;
+  int32_t n_items;
+  int32_t flush_threshold;    // smem table occupancy that triggers a flush to the spill table
+  unsigned int* work_counter; // next item to claim
+  const double* PX;
+  const double* PY;
+  const double* PDZ2;
+  const double* PV;
+  const uint32_t* PKZ;
+  // spill tables: gridDim.x tables of gcap slots each
+  uint64_t* gkeys;
+  unsigned long long* glo;
+  unsigned long long* ghi;
+  uint32_t* gused;
+  unsigned int* gcount;       // gridDim.x counters
+  uint32_t gcap;              // power of two
+  int32_t smem_hist_bins;     // histograms with more bins accumulate straight into HBM
+  // optional export of every sphere (os, key, y); null when not requested
+  SphereRecord* export_buf;
+  unsigned long long* export_count;
+  unsigned long long export_cap;
+  int* error_flags;           // bit 0: spill table full, bit 1: export buffer full
+};
+
+struct PrepareParams {
+  const JobDev* jobs;
+  JobAux* aux;
+  int32_t n_jobs;
+  const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
+  double* PX;
+  double* PY;
+  double* PDZ2;
+  double* PV;
+  uint32_t* PKZ;
+};
+
+constexpr int kPrepThreads = 256;
+constexpr int kPrepSlotsPerBlock = 4 * kWarpTile;
+
+}  // namespace st
