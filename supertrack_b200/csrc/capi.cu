@@ -15,8 +15,8 @@
 
 namespace st {
 cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, cudaStream_t s);
-cudaError_t configure_fused(int smem_hist_bins);
-cudaError_t launch_fused(const FusedParams& p, int grid, cudaStream_t s);
+cudaError_t configure_fused();
+cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
 }  // namespace st
 
@@ -90,7 +90,7 @@ struct st_ctx {
 
   DevBuf track_arena;
   DevBuf px, py, pdz2, pv, pkz;
-  DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err;
+  DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off;
   DevBuf g_keys, g_lo, g_hi, g_used, g_count;
   uint32_t gcap = 0;
   int ggrid = 0;
@@ -119,6 +119,7 @@ struct st_ctx {
   int64_t cache_blocks = 0;
   int cache_grid = 0;
   int64_t cache_arena_total = 0;
+  int cache_max_nbins = 0;
 };
 
 namespace {
@@ -231,6 +232,10 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     D.denom = (2. / 3.) * J.g.sphereDiameter;
     D.zsh = J.desc.zshift == ST_ZSHIFT_PLUS ? J.g.scoringRegionHalfLength
           : J.desc.zshift == ST_ZSHIFT_MINUS ? -J.g.scoringRegionHalfLength : 0.0;
+    // with shifts in (-HL', HL'] a deposit at |x| >= 2HL'(1+2^-30) stays outside the voxel;
+    // without shifts (x + 0 = x) the box test itself decides
+    D.xy_keep = J.desc.shift_track ? 2.0 * J.g.scoringRegionHalfLength * (1.0 + 0x1p-30)
+                                   : J.g.scoringRegionHalfLength;
     D.N = (uint32_t)J.g.numSpheresLinear;
     D.N2 = (uint64_t)D.N * (uint64_t)D.N;
     D.seed = J.desc.seed;
@@ -250,7 +255,22 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     hd[h].counts = (unsigned long long*)c->h_counts.p + c->hists[h].off;
     hd[h].yfy = (double*)c->h_yfy.p + c->hists[h].off;
     hd[h].nbins = c->hists[h].nbins;
+    const std::vector<double>& e = c->hists[h].edges;
+    const double lo = e.front(), hi = e.back();
+    if (c->hists[h].type == ST_HIST_LOG && lo > 0) {
+      hd[h].mode = 1;
+      hd[h].ca = std::log2(lo);
+      hd[h].cb = c->hists[h].nbins / (std::log2(hi) - std::log2(lo));
+    } else {
+      hd[h].mode = 0;
+      hd[h].ca = lo;
+      hd[h].cb = c->hists[h].nbins / (hi - lo);
+    }
   }
+  int max_nbins = 0;
+  for (size_t i = 0; i < nj; ++i)
+    max_nbins = std::max(max_nbins, c->hists[c->jobs[first + i].desc.hist_id].nbins);
+  c->cache_max_nbins = max_nbins;
 
   // work items: oversample blocks of roughly item_cost deposit*oversamples, longest first
   std::vector<WorkItem> items;
@@ -278,6 +298,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(ensure(c->d_hists, std::max<size_t>(1, hd.size()) * sizeof(HistDev)), "hist table");
   ST_CUDA(ensure(c->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)), "items");
   ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
+  ST_CUDA(ensure(c->d_blk_count, (size_t)blk[nj] * 4), "prepare block counts");
+  ST_CUDA(ensure(c->d_blk_off, (size_t)blk[nj] * 8), "prepare block offsets");
   ST_CUDA(ensure(c->d_counter, 16), "work counter");
   ST_CUDA(ensure(c->d_err, 16), "error flags");
   ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, jd.data(), nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
@@ -287,16 +309,25 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     ST_CUDA(cudaMemcpyAsync(c->d_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, c->stream), "upload items");
   ST_CUDA(cudaMemcpyAsync(c->d_blk.p, blk.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
 
-  // spill tables
+  // spill tables: one per resident CTA, able to hold every distinct sphere of the largest job;
+  // the number of resident CTAs shrinks if the tables would exceed 30% of free memory
   int grid = c->grid_override > 0 ? c->grid_override : c->sm_count;
   grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)items.size()));
-  const uint32_t gcap = next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024));
+  const uint32_t gcap = std::max(c->gcap, next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024)));
+  {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t have = (size_t)c->gcap * (size_t)c->ggrid * 28;
+    const double budget = std::min(0.3 * (double)(free_b + have), 48e9);
+    const int fit = (int)std::max(1.0, std::floor(budget / ((double)gcap * 28.0)));
+    grid = std::min(grid, fit);
+  }
   if (gcap > c->gcap || grid > c->ggrid || c->g_dirty) {
-    st_status s = init_spill_tables(c, std::max(gcap, c->gcap), std::max(grid, c->ggrid));
+    st_status s = init_spill_tables(c, gcap, grid);
     if (s != ST_OK) return s;
   }
   if (!c->fused_configured) {
-    ST_CUDA(st::configure_fused(c->smem_hist_bins), "configure fused kernel");
+    ST_CUDA(st::configure_fused(), "configure fused kernel");
     c->fused_configured = true;
   }
 
@@ -305,6 +336,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.aux = (JobAux*)c->d_aux.p;
   pp.n_jobs = (int32_t)nj;
   pp.blk_prefix = (const int64_t*)c->d_blk.p;
+  pp.blk_count = (int32_t*)c->d_blk_count.p;
+  pp.blk_offset = (int64_t*)c->d_blk_off.p;
   pp.PX = (double*)c->px.p;
   pp.PY = (double*)c->py.p;
   pp.PDZ2 = (double*)c->pdz2.p;
@@ -376,7 +409,7 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
   ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->stream), "prepare launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
-  ST_CUDA(st::launch_fused(fp, c->cache_grid, c->stream), "fused launch");
+  ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->stream), "fused launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
   c->launches += (c->cache_blocks > 0 ? 1 : 0) + (c->cache_grid > 0 ? 1 : 0);
 
@@ -556,7 +589,7 @@ st_status st_ctx_destroy(st_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pv, &c->pkz,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
-                    &c->d_counter, &c->d_err, &c->g_keys, &c->g_lo, &c->g_hi,
+                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};
   for (DevBuf* b : bufs) release(*b);

@@ -2,7 +2,8 @@
 //
 // HBM layout of one batch:
 //   * input tracks: SoA float64 x, y, z, edep per job (caller memory or the context's arena);
-//   * prepared arena (written once per job, read once per oversample): for every job a padded
+//   * prepared arena (written once per job, read once per oversample): for every job its kept
+//     deposits (those that can lie inside the voxel for some shift; order preserved) as a padded
 //     run of warp tiles of kWarpTile deposits, stored tile by tile in "lane-blocked" order so a
 //     warp-wide load of row p reads 32 consecutive doubles while lane l owns the kDepPerLane
 //     consecutive deposits l*kDepPerLane .. l*kDepPerLane+kDepPerLane-1 of the tile:
@@ -39,6 +40,7 @@ struct JobDev {
   double r2;          // RN(r*r)
   double denom;       // RN(RN(2/3)*d): lineal-energy denominator
   double zsh;         // z-origin shift added to every z
+  double xy_keep;     // |x|, |y| at or beyond this can never be inside the voxel after a shift
   uint64_t N2;        // N*N
   uint64_t seed;
   uint64_t track_id;
@@ -54,6 +56,7 @@ struct JobAux {
   int32_t e_max;          // max ulp exponent over nonzero contributions
   int32_t flags;          // kAuxNonzero | kAuxNonfinite
   int32_t pad;
+  long long kept;              // deposits that can be inside the voxel for some shift
   unsigned long long hits;     // in-sphere deposits summed over all oversamples
   unsigned long long spheres;  // (oversample, sphere) pairs with at least one hit
   unsigned long long binned;   // of those, the ones that landed inside the histogram range
@@ -67,7 +70,8 @@ struct HistDev {
   unsigned long long* counts;     // nbins
   double* yfy;                    // nbins
   int32_t nbins;
-  int32_t pad;
+  int32_t mode;                   // bin guess: 0 linear in y, 1 linear in log2(y)
+  double ca, cb;                  // guess = (y - ca) * cb  or  (log2(y) - ca) * cb
 };
 
 // One unit of work for the persistent kernel: a contiguous block of oversamples of one job.
@@ -119,6 +123,8 @@ struct PrepareParams {
   JobAux* aux;
   int32_t n_jobs;
   const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
+  int32_t* blk_count;         // kept deposits per prepare block
+  int64_t* blk_offset;        // first kept index of each prepare block inside its job
   double* PX;
   double* PY;
   double* PDZ2;

@@ -1,9 +1,10 @@
 // sm_100a kernels of the VoxelConstrainedSphere superimposition path.
 //
-//   k_prepare : once per track. z-origin shift, z-box test, the z part of the lattice test
-//               (k_z and (k_z*d - a_z)^2, which do not depend on the oversample), the lineal
-//               energy contribution v = edep/((2/3)d), the job's fixed-point exponent range, and
-//               the lane-blocked relayout of the deposits into the prepared arena.
+//   prepare   : once per track (k_prep_count/scan/write/pad). z-origin shift, the deposits that
+//               can be in the voxel for some shift, the z part of the lattice test (k_z and
+//               (k_z*d - a_z)^2, which do not depend on the oversample), the lineal energy
+//               contribution v = edep/((2/3)d), the job's fixed-point exponent range, and the
+//               ordered, lane-blocked compaction of the kept deposits into the prepared arena.
 //               Follows VoxelConstrainedSphereMethod.cu:138-154 (z shift), :198 (|z| test),
 //               :249-258 (z axis of the membership test), :302/:322 (lineal denominator).
 //   k_fused   : persistent work-stealing kernel over (job, oversample block) items. Per
@@ -45,71 +46,178 @@ __device__ __forceinline__ void lattice_index(double a, double d, double inv_d, 
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_prepare
+// Prepare stage (once per track): four launches.
+//   k_prep_count : per block of kPrepSlotsPerBlock source deposits, the number of deposits that
+//                  can lie inside the voxel for some oversample (z after the z-origin shift
+//                  strictly inside; |x|, |y| below xy_keep), plus the job's exponent range of
+//                  the contributions v = edep/((2/3)d) over all its deposits;
+//   k_prep_scan  : per job, exclusive scan of its block counts -> block offsets, kept total;
+//   k_prep_write : ordered compaction of the kept deposits into the lane-blocked arena with
+//                  the oversample-independent z part of the lattice test;
+//   k_prep_pad   : padding of each job's last warp tile (NaN x so the box test rejects it).
+// A dropped deposit can be inside the box for no shift, so dropping it changes no result.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPrepThreads) k_prepare(PrepareParams p) {
-  const int64_t b = blockIdx.x;
-  int lo = 0, hi = p.n_jobs;
+__device__ __forceinline__ int find_job(const int64_t* blk_prefix, int n_jobs, int64_t b) {
+  int lo = 0, hi = n_jobs;
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
-    if (p.blk_prefix[mid] <= b) lo = mid; else hi = mid;
+    if (blk_prefix[mid] <= b) lo = mid; else hi = mid;
   }
-  const int j = lo;
+  return lo;
+}
+
+__device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y, double z) {
+  const double z1 = st_dadd(z, J.zsh);
+  return fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
+}
+
+__global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
+  const int64_t b = blockIdx.x;
+  const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
-  const int64_t local0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
-  int emin = INT_MAX, emax = INT_MIN, flags = 0;
-  const double nan = __longlong_as_double(0x7FF8000000000000ll);
-  const double inf = __longlong_as_double(0x7FF0000000000000ll);
+  const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
+  int emin = INT_MAX, emax = INT_MIN, flags = 0, kept = 0;
   for (int s = threadIdx.x; s < kPrepSlotsPerBlock; s += kPrepThreads) {
-    const int64_t t = local0 + s;
-    if (t >= J.n_pad) break;
-    const int64_t w = t / kWarpTile;
-    const int rem = (int)(t - w * kWarpTile);
-    const int pp = rem >> 5, lane = rem & 31;
-    const int64_t i = w * kWarpTile + lane * kDepPerLane + pp;
-    double px = nan, py = nan, dz2 = inf, v = 0.0;
-    uint32_t kz = 0;
-    if (i < J.n) {
-      px = J.x[i];
-      py = J.y[i];
-      const double z1 = st_dadd(J.z[i], J.zsh);
-      if (fabs(z1) < J.HL) {
-        const double az = st_dsub(z1, J.gSO);
-        const double kd = rint(__ddiv_rn(az, J.d));
-        const double dz = st_dsub(st_dmul(kd, J.d), az);
-        dz2 = st_dmul(dz, dz);
-        kz = (uint32_t)(long long)kd;
-      }
-      v = __ddiv_rn(J.edep[i], J.denom);
-      if (!isfinite(v)) {
-        flags |= kAuxNonfinite;
-      } else if (v != 0.0) {
-        flags |= kAuxNonzero;
-        const int ex = ulp_exponent(v);
-        emin = min(emin, ex);
-        emax = max(emax, ex);
-      }
+    const int64_t i = i0 + s;
+    if (i >= J.n) break;
+    kept += keep_deposit(J, J.x[i], J.y[i], J.z[i]) ? 1 : 0;
+    const double v = __ddiv_rn(J.edep[i], J.denom);
+    if (!isfinite(v)) {
+      flags |= kAuxNonfinite;
+    } else if (v != 0.0) {
+      flags |= kAuxNonzero;
+      const int ex = ulp_exponent(v);
+      emin = min(emin, ex);
+      emax = max(emax, ex);
     }
-    const int64_t dst = J.prep_off + t;
-    p.PX[dst] = px;
-    p.PY[dst] = py;
-    p.PDZ2[dst] = dz2;
-    p.PV[dst] = v;
-    p.PKZ[dst] = kz;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     emin = min(emin, __shfl_xor_sync(0xffffffffu, emin, o));
     emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
     flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+    kept += __shfl_xor_sync(0xffffffffu, kept, o);
   }
-  if ((threadIdx.x & 31) == 0 && flags) {
-    atomicOr(&p.aux[j].flags, flags);
-    if (flags & kAuxNonzero) {
-      atomicMin(&p.aux[j].e_min, emin);
-      atomicMax(&p.aux[j].e_max, emax);
+  __shared__ int s_kept;
+  if (threadIdx.x == 0) s_kept = 0;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&s_kept, kept);
+    if (flags) {
+      atomicOr(&p.aux[j].flags, flags);
+      if (flags & kAuxNonzero) {
+        atomicMin(&p.aux[j].e_min, emin);
+        atomicMax(&p.aux[j].e_max, emax);
+      }
     }
   }
+  __syncthreads();
+  if (threadIdx.x == 0) p.blk_count[b] = s_kept;
+}
+
+// One CTA per job: exclusive scan of the job's block counts.
+__global__ void __launch_bounds__(1024) k_prep_scan(PrepareParams p) {
+  const int j = blockIdx.x;
+  const int64_t b0 = p.blk_prefix[j], nb = p.blk_prefix[j + 1] - b0;
+  __shared__ long long s_warp[32];
+  __shared__ long long s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t base = 0; base < nb; base += 1024) {
+    const int64_t k = base + threadIdx.x;
+    long long v = k < nb ? p.blk_count[b0 + k] : 0;
+    long long incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      long long w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const long long warp_base = warp ? s_warp[warp - 1] : 0;
+    if (k < nb) p.blk_offset[b0 + k] = s_carry + warp_base + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) p.aux[j].kept = s_carry;
+}
+
+__global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
+  const int64_t b = blockIdx.x;
+  const int j = find_job(p.blk_prefix, p.n_jobs, b);
+  const JobDev J = p.jobs[j];
+  const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarpsPerBlock = kPrepThreads / 32;
+  __shared__ int s_warp[kWarpsPerBlock];
+  int64_t run = p.blk_offset[b];  // kept index of the next kept deposit of this block
+  for (int r = 0; r < kPrepSlotsPerBlock / kPrepThreads; ++r) {
+    const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
+    bool keep = false;
+    double x = 0, y = 0, z1 = 0;
+    if (i < J.n) {
+      x = J.x[i];
+      y = J.y[i];
+      z1 = st_dadd(J.z[i], J.zsh);
+      keep = fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) s_warp[warp] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < kWarpsPerBlock; ++w) {
+      const int c = s_warp[w];
+      before += (w < warp) ? c : 0;
+      total += c;
+    }
+    if (keep) {
+      const int64_t k = run + before + __popc(m & ((1u << lane) - 1u));
+      const double az = st_dsub(z1, J.gSO);
+      const double kd = rint(__ddiv_rn(az, J.d));
+      const double dz = st_dsub(st_dmul(kd, J.d), az);
+      const int64_t w = k / kWarpTile;
+      const int rem = (int)(k - w * kWarpTile);
+      const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+      p.PX[dst] = x;
+      p.PY[dst] = y;
+      p.PDZ2[dst] = st_dmul(dz, dz);
+      p.PV[dst] = __ddiv_rn(J.edep[i], J.denom);
+      p.PKZ[dst] = (uint32_t)(long long)kd;
+    }
+    run += total;
+    __syncthreads();
+  }
+}
+
+// One block per job: padding slots [kept, kept rounded up to a warp tile).
+__global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
+  const int j = blockIdx.x;
+  const JobDev J = p.jobs[j];
+  const long long kept = p.aux[j].kept;
+  if ((kept % kWarpTile) == 0) return;
+  const long long k = kept + threadIdx.x;
+  if (k >= (kept / kWarpTile + 1) * kWarpTile) return;
+  const int64_t w = k / kWarpTile;
+  const int rem = (int)(k - w * kWarpTile);
+  const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+  p.PX[dst] = __longlong_as_double(0x7FF8000000000000ll);
+  p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
+  p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
+  p.PV[dst] = 0.0;
+  p.PKZ[dst] = 0;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -165,15 +273,25 @@ struct CtaState {
   int item;
   int tcount;
   int spilled;
+  int edges_hist;   // histogram whose edges are in shared memory (-1: none)
+};
+
+// Spill table of the current item: the CTA's table restricted to a power-of-two prefix sized
+// for the item's job, so that small jobs touch a small, cache-friendly region.
+struct Spill {
+  uint64_t* keys;
+  unsigned long long* lo;
+  unsigned long long* hi;
+  uint32_t* used;
+  unsigned int* count;
+  uint32_t cap;
 };
 
 // Adds one sphere contribution to the CTA's shared-memory table, or to the spill table when the
-// shared table is at its load limit.
+// shared table is at its load limit or the probe sequence is too long.
 template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
-                                           const FusedParams& P, uint64_t* gk,
-                                           unsigned long long* glo, unsigned long long* ghi,
-                                           uint32_t* gused, unsigned int* gcnt, uint64_t key,
+                                           const FusedParams& P, const Spill& G, uint64_t key,
                                            uint64_t lo, uint64_t hi) {
   constexpr int kHardLimit = (CAP * 3) / 4;
   if (*(volatile int*)&cs->tcount < kHardLimit) {
@@ -196,20 +314,46 @@ __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs
     }
   }
   *(volatile int*)&cs->spilled = 1;
-  if (!gtable_add(gk, glo, ghi, gused, gcnt, P.gcap, key, lo, hi)) atomicOr(P.error_flags, 1);
+  if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, key, lo, hi))
+    atomicOr(P.error_flags, 1);
 }
 
 struct BinContext {
-  const double* edges;
+  const double* edges;    // shared-memory copy when the histogram fits, else HBM
   unsigned long long* gcounts;
   double* gyfy;
   unsigned int* hcount;   // null: accumulate straight into HBM
   double* hyfy;
   int nbins;
+  int mode;               // 0: linear candidate, 1: log2 candidate
+  double ca, cb;          // candidate bin = (y - ca) * cb, or (log2 y - ca) * cb
   int E0;
   int os;
   int job;
 };
+
+// HistogramRange bin of y (edges[b] <= y < edges[b+1], else -1). An arithmetic guess of the
+// bin is corrected against the exact edges, so the result is the same as a binary search.
+__device__ __forceinline__ int find_bin_fast(const BinContext& B, double y) {
+  const double* e = B.edges;
+  const int nb = B.nbins;
+  if (!(y >= e[0]) || !(y < e[nb])) return -1;
+  const float t = B.mode ? (__log2f((float)y) - (float)B.ca) * (float)B.cb
+                         : (float)((y - B.ca) * B.cb);
+  int b = (t >= 0.f) ? (t < (float)nb ? (int)t : nb - 1) : 0;
+#pragma unroll 1
+  for (int it = 0; it < 8; ++it) {
+    if (y < e[b]) { --b; continue; }
+    if (y >= e[b + 1]) { ++b; continue; }
+    return b;
+  }
+  int l = 0, h = nb;  // far-off guess: binary search
+  while (h - l > 1) {
+    const int m = (l + h) >> 1;
+    if (e[m] <= y) l = m; else h = m;
+  }
+  return l;
+}
 
 __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParams& P,
                                            uint64_t key, uint64_t lo, uint64_t hi,
@@ -217,21 +361,7 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
                                            unsigned long long& binned) {
   const double y = from_fixed(lo, hi, B.E0);
   ++spheres;
-  int b;
-  {
-    // HistogramRange: edges[b] <= y < edges[b+1]
-    const double* e = B.edges;
-    if (!(y >= __ldg(&e[0])) || !(y < __ldg(&e[B.nbins]))) {
-      b = -1;
-    } else {
-      int l = 0, h = B.nbins;
-      while (h - l > 1) {
-        const int m = (l + h) >> 1;
-        if (__ldg(&e[m]) <= y) l = m; else h = m;
-      }
-      b = l;
-    }
-  }
+  const int b = find_bin_fast(B, y);
   if (b >= 0) {
     ++binned;
     if (B.hcount) {
@@ -257,6 +387,20 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
   }
 }
 
+// Moves every shared-memory entry into the spill table and empties the shared table.
+template <int CAP, int THREADS>
+__device__ __forceinline__ void flush_to_spill(const SmemTable<CAP>& T, int cnt,
+                                               const FusedParams& P, const Spill& G) {
+  for (int i = threadIdx.x; i < cnt; i += THREADS) {
+    const uint32_t h = T.used[i];
+    if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
+      atomicOr(P.error_flags, 1);
+    T.keys[h] = kEmptyKey;
+    T.lo[h] = 0;
+    T.hi[h] = 0;
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // k_fused
 // ---------------------------------------------------------------------------------------------
@@ -267,32 +411,35 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ CtaState cs;
 
+  const int HB = P.smem_hist_bins;
   SmemTable<CAP> T;
   T.keys = reinterpret_cast<uint64_t*>(smem_raw);
   T.lo = reinterpret_cast<unsigned long long*>(T.keys + CAP);
   T.hi = T.lo + CAP;
   double* hyfy = reinterpret_cast<double*>(T.hi + CAP);
-  unsigned int* hcount = reinterpret_cast<unsigned int*>(hyfy + P.smem_hist_bins);
-  T.used = reinterpret_cast<uint16_t*>(hcount + P.smem_hist_bins);
+  double* sedges = hyfy + HB;                                   // HB + 1 edges
+  unsigned int* hcount = reinterpret_cast<unsigned int*>(sedges + HB + 1);
+  T.used = reinterpret_cast<uint16_t*>(hcount + HB);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  uint64_t* gk = P.gkeys + (size_t)blockIdx.x * P.gcap;
-  unsigned long long* glo = P.glo + (size_t)blockIdx.x * P.gcap;
-  unsigned long long* ghi = P.ghi + (size_t)blockIdx.x * P.gcap;
-  uint32_t* gused = P.gused + (size_t)blockIdx.x * P.gcap;
+  uint64_t* gk_base = P.gkeys + (size_t)blockIdx.x * P.gcap;
+  unsigned long long* glo_base = P.glo + (size_t)blockIdx.x * P.gcap;
+  unsigned long long* ghi_base = P.ghi + (size_t)blockIdx.x * P.gcap;
+  uint32_t* gused_base = P.gused + (size_t)blockIdx.x * P.gcap;
   unsigned int* gcnt = P.gcount + blockIdx.x;
 
   for (int i = tid; i < CAP; i += THREADS) { T.keys[i] = kEmptyKey; T.lo[i] = 0; T.hi[i] = 0; }
-  for (int i = tid; i < P.smem_hist_bins; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
-  if (tid == 0) { cs.tcount = 0; cs.spilled = 0; }
+  for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
+  if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.edges_hist = -1; }
   __syncthreads();
 
   for (;;) {
     if (tid == 0) cs.item = (int)atomicAdd(P.work_counter, 1u);
     __syncthreads();
     const int it = cs.item;
+    const int cached_hist = cs.edges_hist;
     __syncthreads();
     if (it >= P.n_items) break;
 
@@ -302,21 +449,42 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     if (A.flags & kAuxNonfinite) continue;  // rejected job: contributes nothing, host reports it
     const HistDev H = P.hists[J.hist];
     const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
+    const bool smem_hist = H.nbins <= HB;
+
+    // histogram edges into shared memory (kept while consecutive items use the same histogram)
+    if (smem_hist && cached_hist != J.hist) {
+      for (int i = tid; i <= H.nbins; i += THREADS) sedges[i] = H.edges[i];
+      __syncthreads();
+      if (tid == 0) cs.edges_hist = J.hist;
+    }
 
     BinContext B;
-    B.edges = H.edges;
+    B.edges = smem_hist ? sedges : H.edges;
     B.gcounts = H.counts;
     B.gyfy = H.yfy;
     B.nbins = H.nbins;
+    B.mode = H.mode;
+    B.ca = H.ca;
+    B.cb = H.cb;
     B.E0 = E0;
     B.job = W.job;
-    const bool smem_hist = H.nbins <= P.smem_hist_bins;
     B.hcount = smem_hist ? hcount : nullptr;
     B.hyfy = smem_hist ? hyfy : nullptr;
 
-    const int64_t n_wt = J.n_pad / kWarpTile;
+    Spill G;
+    G.keys = gk_base;
+    G.lo = glo_base;
+    G.hi = ghi_base;
+    G.used = gused_base;
+    G.count = gcnt;
+    {
+      uint32_t cap = 1024;
+      while (cap < P.gcap && (long long)cap < 2 * A.kept) cap <<= 1;
+      G.cap = cap;
+    }
+
+    const int64_t n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
     unsigned long long hits = 0, spheres = 0, binned = 0, inbox = 0;
-    const double kInf = __longlong_as_double(0x7FF0000000000000ll);
 
     for (int os = W.os_begin; os < W.os_begin + W.os_count; ++os) {
       float ux, uy;
@@ -342,20 +510,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
           for (int p = 0; p < kDepPerLane; ++p) {
             const double x1 = st_dadd(xv[p], sx);
             const double y1 = st_dadd(yv[p], sy);
-            const double ax = st_dsub(x1, J.gSO);
-            const double ay = st_dsub(y1, J.gSO);
-            double kdx, kdy;
-            lattice_index(ax, J.d, J.inv_d, kxv[p], kdx);
-            lattice_index(ay, J.d, J.inv_d, kyv[p], kdy);
-            const double ddx = st_dsub(st_dmul(kdx, J.d), ax);
-            const double ddy = st_dsub(st_dmul(kdy, J.d), ay);
-            const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dv[p]);
-            const bool inbox = fabs(x1) < J.HL && fabs(y1) < J.HL && dv[p] != kInf;
-            if (inbox) boxmask |= 1u << p;
-            if (inbox && dist <= J.r2) hitmask |= 1u << p;
+            kxv[p] = 0;
+            kyv[p] = 0;
+            if (fabs(x1) < J.HL && fabs(y1) < J.HL) {
+              boxmask |= 1u << p;
+              const double ax = st_dsub(x1, J.gSO);
+              const double ay = st_dsub(y1, J.gSO);
+              double kdx, kdy;
+              lattice_index(ax, J.d, J.inv_d, kxv[p], kdx);
+              lattice_index(ay, J.d, J.inv_d, kyv[p], kdy);
+              const double ddx = st_dsub(st_dmul(kdx, J.d), ax);
+              const double ddy = st_dsub(st_dmul(kdy, J.d), ay);
+              const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dv[p]);
+              if (dist <= J.r2) hitmask |= 1u << p;
+            }
           }
           hits += __popc(hitmask);
           inbox += __popc(boxmask);
+          // runs of equal keys inside the lane's consecutive deposits are summed in registers
           uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
 #pragma unroll
           for (int p = 0; p < kDepPerLane; ++p) {
@@ -370,23 +542,35 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
               if (key == rkey) {
                 add128(rlo, rhi, lo, hi);
               } else {
-                if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, gk, glo, ghi, gused, gcnt, rkey, rlo, rhi);
+                if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi);
                 rkey = key; rlo = lo; rhi = hi;
               }
             }
           }
-          if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, gk, glo, ghi, gused, gcnt, rkey, rlo, rhi);
+          // the lanes' last runs: segmented sum over consecutive lanes with the same key, so a
+          // sphere spanning several lanes costs one shared-memory update
+          {
+            const uint64_t kprev = __shfl_up_sync(0xffffffffu, rkey, 1);
+            const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
+            bool head = lane == 0 || kprev != rkey;
+            const bool tail = lane == 31 || knext != rkey;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
+              const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
+              const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
+              if (lane >= o && !head) {
+                add128(rlo, rhi, olo, ohi);
+                head = ohead;
+              }
+            }
+            if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi);
+          }
         }
         if (wt0 + kWarps < n_wt) {
           __syncthreads();
           if (cs.tcount > P.flush_threshold) {
-            const int cnt = cs.tcount;
-            for (int i = tid; i < cnt; i += THREADS) {
-              const uint32_t h = T.used[i];
-              if (!gtable_add(gk, glo, ghi, gused, gcnt, P.gcap, T.keys[h], T.lo[h], T.hi[h]))
-                atomicOr(P.error_flags, 1);
-              T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
-            }
+            flush_to_spill<CAP, THREADS>(T, cs.tcount, P, G);
             __syncthreads();
             if (tid == 0) { cs.tcount = 0; cs.spilled = 1; }
             __syncthreads();
@@ -398,24 +582,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       // ---- reduce-by-key complete for this oversample: bin every sphere
       const int cnt = cs.tcount;
       if (cs.spilled) {
-        for (int i = tid; i < cnt; i += THREADS) {
-          const uint32_t h = T.used[i];
-          if (!gtable_add(gk, glo, ghi, gused, gcnt, P.gcap, T.keys[h], T.lo[h], T.hi[h]))
-            atomicOr(P.error_flags, 1);
-          T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
-        }
+        flush_to_spill<CAP, THREADS>(T, cnt, P, G);
         __syncthreads();
-        const unsigned gc = __ldcg(gcnt);
+        const unsigned gc = __ldcg(G.count);
         for (unsigned i = tid; i < gc; i += THREADS) {
-          const uint32_t h = __ldcg(&gused[i]);
-          const uint64_t key = __ldcg((const unsigned long long*)&gk[h]);
-          const uint64_t lo = __ldcg(&glo[h]);
-          const uint64_t hi = __ldcg(&ghi[h]);
+          const uint32_t h = __ldcg(&G.used[i]);
+          const uint64_t key = __ldcg((const unsigned long long*)&G.keys[h]);
+          const uint64_t lo = __ldcg(&G.lo[h]);
+          const uint64_t hi = __ldcg(&G.hi[h]);
           bin_sphere(B, P, key, lo, hi, spheres, binned);
-          gk[h] = kEmptyKey; glo[h] = 0; ghi[h] = 0;
+          G.keys[h] = kEmptyKey; G.lo[h] = 0; G.hi[h] = 0;
         }
         __syncthreads();
-        if (tid == 0) *gcnt = 0;
+        if (tid == 0) *G.count = 0;
       } else {
         for (int i = tid; i < cnt; i += THREADS) {
           const uint32_t h = T.used[i];
@@ -484,28 +663,51 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------------------------
 constexpr int kFusedThreads = 512;
-constexpr int kSmemCap = 4096;
 
-size_t fused_smem_bytes(int smem_hist_bins) {
-  return (size_t)kSmemCap * 24 + (size_t)smem_hist_bins * 12 + (size_t)kSmemCap * 2;
+// Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
+// 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
+// most kSmallHistBins bins.
+constexpr int kSmallHistBins = 768;
+constexpr int kBigHistBins = 4096;
+
+size_t fused_smem_bytes(int cap, int hist_bins) {
+  return (size_t)cap * 26 + (size_t)hist_bins * 20 + 8;
 }
 
 cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, cudaStream_t s) {
   if (n_blocks <= 0) return cudaSuccess;
-  k_prepare<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
+  k_prep_count<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
+  k_prep_scan<<<p.n_jobs, 1024, 0, s>>>(p);
+  k_prep_write<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
+  k_prep_pad<<<p.n_jobs, kWarpTile, 0, s>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t configure_fused(int smem_hist_bins) {
-  return cudaFuncSetAttribute(k_fused<kSmemCap, kFusedThreads>,
+cudaError_t configure_fused() {
+  cudaError_t e = cudaFuncSetAttribute(k_fused<4096, kFusedThreads>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)fused_smem_bytes(4096, kBigHistBins));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fused<8192, kFusedThreads>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)fused_smem_bytes(smem_hist_bins));
+                              (int)fused_smem_bytes(8192, kSmallHistBins));
 }
 
-cudaError_t launch_fused(const FusedParams& p, int grid, cudaStream_t s) {
+// Picks the kernel shape from the largest histogram of the batch; fills P.smem_hist_bins and
+// P.flush_threshold.
+cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
-  k_fused<kSmemCap, kFusedThreads>
-      <<<grid, kFusedThreads, fused_smem_bytes(p.smem_hist_bins), s>>>(p);
+  if (max_nbins <= kSmallHistBins) {
+    p.smem_hist_bins = kSmallHistBins;
+    p.flush_threshold = 8192 / 2;
+    k_fused<8192, kFusedThreads>
+        <<<grid, kFusedThreads, fused_smem_bytes(8192, kSmallHistBins), s>>>(p);
+  } else {
+    p.smem_hist_bins = kBigHistBins;
+    p.flush_threshold = 4096 / 2;
+    k_fused<4096, kFusedThreads>
+        <<<grid, kFusedThreads, fused_smem_bytes(4096, kBigHistBins), s>>>(p);
+  }
   return cudaGetLastError();
 }
 

@@ -70,15 +70,14 @@ def test_config4_scaled_dense_spill(ctx):
 
 
 def test_sparse_spill_many_spheres(ctx):
-    """2 nm spheres over a long sparse track: tens of thousands of distinct spheres per
-    oversample (shared table flushes repeatedly)."""
-    w = W.config0(n_tracks=2, n_dep=150_000, n_os=2)
-    w.diameter[:] = 2.0
+    """2 nm spheres over a dense ion track: tens of thousands of distinct spheres per
+    oversample, far more than the shared-memory table holds (repeated flushes to HBM)."""
+    w = W.config1(n_tracks=1, n_dep=300_000, n_os=2)
     gc, gy, gs, _ = gpu_run(ctx, w)
     oc, oy, os_, _ = oracle_run(w)
     assert_stats_equal(gs, os_)
     assert_hist_equal(gc, gy, oc, oy)
-    assert gs[0]["spheres"] > 20000
+    assert gs[0]["spheres"] > 2 * 40000
 
 
 def test_batched_plain_and_alone_agree(ctx):
