@@ -14,7 +14,8 @@
 #include "st_device.cuh"
 
 namespace st {
-cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, cudaStream_t s);
+cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_flagged,
+                           cudaStream_t s);
 cudaError_t configure_fused();
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
@@ -91,6 +92,7 @@ struct st_ctx {
   DevBuf track_arena;
   DevBuf px, py, pdz2, pv, pkz;
   DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off;
+  DevBuf c_keys, c_min, c_max, pz;   // cell arena and shifted z of flagged jobs
   DevBuf g_keys, g_lo, g_hi, g_used, g_count;
   uint32_t gcap = 0;
   int ggrid = 0;
@@ -120,6 +122,8 @@ struct st_ctx {
   int cache_grid = 0;
   int64_t cache_arena_total = 0;
   int cache_max_nbins = 0;
+  int64_t cache_cells = 0;
+  bool cache_any_flagged = false;
 };
 
 namespace {
@@ -209,6 +213,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   std::vector<JobDev> jd(nj);
   std::vector<JobAux> aux(nj);
   std::vector<int64_t> blk(nj + 1, 0);
+  int64_t cells_total = 0;
+  bool any_flagged = false;
   for (size_t i = 0; i < nj; ++i) {
     JobHost& J = c->jobs[first + i];
     JobDev& D = jd[i];
@@ -243,6 +249,18 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     D.n_os = (int32_t)J.desc.n_oversamples;
     D.shift_track = J.desc.shift_track ? 1 : 0;
     D.hist = J.desc.hist_id;
+    // boundary flags pay off for multi-window jobs on fine lattices with several oversamples
+    D.flagged = (J.track.n > 2 * st::kWindow && J.desc.n_oversamples >= 4 &&
+                 D.N >= 128 && D.N < (1u << (st::kCellBits - 2))) ? 1 : 0;
+    D.cell_cap = 0;
+    D.cell_off = 0;
+    D.cell_size = J.g.sphereDiameter * (1.0 + 0x1p-10);
+    if (D.flagged) {
+      D.cell_cap = next_pow2((uint64_t)2 * (uint64_t)J.track.n);
+      D.cell_off = cells_total;
+      cells_total += D.cell_cap;
+      any_flagged = true;
+    }
     JobAux& A = aux[i];
     std::memset(&A, 0, sizeof(A));
     A.e_min = 0x7fffffff;
@@ -299,6 +317,10 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(ensure(c->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)), "items");
   ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
   ST_CUDA(ensure(c->d_blk_count, (size_t)blk[nj] * 4), "prepare block counts");
+  ST_CUDA(ensure(c->c_keys, (size_t)cells_total * 8), "cell arena");
+  ST_CUDA(ensure(c->c_min, (size_t)cells_total * 4), "cell arena");
+  ST_CUDA(ensure(c->c_max, (size_t)cells_total * 4), "cell arena");
+  ST_CUDA(ensure(c->pz, any_flagged ? (size_t)prep_total * 8 : 16), "shifted z");
   ST_CUDA(ensure(c->d_blk_off, (size_t)blk[nj] * 8), "prepare block offsets");
   ST_CUDA(ensure(c->d_counter, 16), "work counter");
   ST_CUDA(ensure(c->d_err, 16), "error flags");
@@ -338,6 +360,10 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.blk_prefix = (const int64_t*)c->d_blk.p;
   pp.blk_count = (int32_t*)c->d_blk_count.p;
   pp.blk_offset = (int64_t*)c->d_blk_off.p;
+  pp.ckeys = (uint64_t*)c->c_keys.p;
+  pp.cmin = (uint32_t*)c->c_min.p;
+  pp.cmax = (uint32_t*)c->c_max.p;
+  pp.PZ = (double*)c->pz.p;
   pp.PX = (double*)c->px.p;
   pp.PY = (double*)c->py.p;
   pp.PDZ2 = (double*)c->pdz2.p;
@@ -369,6 +395,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   c->cache_blocks = blk[nj];
   c->cache_grid = items.empty() ? 0 : grid;
   c->cache_arena_total = arena_total;
+  c->cache_cells = cells_total;
+  c->cache_any_flagged = any_flagged;
   c->cache_first = first;
   c->cache_last = last;
   c->cache_valid = !want_export;
@@ -394,6 +422,11 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   }
   ST_CUDA(cudaMemcpyAsync(c->d_aux.p, c->cache_aux.data(), nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
   ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
+  if (c->cache_cells > 0) {
+    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+  }
   ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
 
   st::FusedParams fp = c->cache_fp;
@@ -407,7 +440,7 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   }
 
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
-  ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->stream), "prepare launch");
+  ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->cache_any_flagged, c->stream), "prepare launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
   ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->stream), "fused launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
@@ -589,7 +622,8 @@ st_status st_ctx_destroy(st_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pv, &c->pkz,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
-                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->g_keys, &c->g_lo, &c->g_hi,
+                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->c_keys,
+                    &c->c_min, &c->c_max, &c->pz, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};
   for (DevBuf* b : bufs) release(*b);

@@ -48,7 +48,18 @@ struct JobDev {
   int32_t n_os;
   int32_t shift_track;
   int32_t hist;       // histogram index
+  // boundary flags (see k_prep_flag): computed when `flagged`; the cell hash of the job lives in
+  // the cell arena at [cell_off, cell_off + cell_cap)
+  int32_t flagged;
+  uint32_t cell_cap;
+  int64_t cell_off;
+  double cell_size;
 };
+
+// Deposits are processed in windows of kWindow consecutive kept deposits (one CTA tile of the
+// fused kernel). A kept deposit is a boundary deposit when a kept deposit of another window lies
+// within distance d of it; the flag travels in the top bit of its PKZ word.
+constexpr uint32_t kBoundaryBit = 0x80000000u;
 
 // Per-job values produced on the device.
 struct JobAux {
@@ -125,6 +136,10 @@ struct PrepareParams {
   const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
   int32_t* blk_count;         // kept deposits per prepare block
   int64_t* blk_offset;        // first kept index of each prepare block inside its job
+  uint64_t* ckeys;            // cell arena: cell key, EMPTY when free
+  uint32_t* cmin;             // smallest window with a deposit in the cell
+  uint32_t* cmax;             // largest window with a deposit in the cell
+  double* PZ;                 // z after the z-origin shift (flagged jobs only)
   double* PX;
   double* PY;
   double* PDZ2;
@@ -134,5 +149,8 @@ struct PrepareParams {
 
 constexpr int kPrepThreads = 256;
 constexpr int kPrepSlotsPerBlock = 4 * kWarpTile;
+constexpr int kFusedWarps = 16;                       // warps of the fused kernel's CTA
+constexpr int kWindow = kFusedWarps * kWarpTile;      // kept deposits per window
+constexpr int kCellBits = 21;                         // bits per axis of a cell key
 
 }  // namespace st

@@ -71,6 +71,52 @@ __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y
   return fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
 }
 
+// Cell of side cell_size (slightly above d) containing (x, y, z), offset by (dx, dy, dz) cells.
+// Two deposits within distance d of each other lie in the same or in adjacent cells.
+__device__ __forceinline__ uint64_t cell_key(double x, double y, double z, double cs, int dx,
+                                             int dy, int dz) {
+  const long long off = 1ll << (kCellBits - 1);
+  const uint64_t cx = (uint64_t)((long long)floor(__ddiv_rn(x, cs)) + off + dx);
+  const uint64_t cy = (uint64_t)((long long)floor(__ddiv_rn(y, cs)) + off + dy);
+  const uint64_t cz = (uint64_t)((long long)floor(__ddiv_rn(z, cs)) + off + dz);
+  return (cz << (2 * kCellBits)) | (cy << kCellBits) | cx;
+}
+
+__device__ __forceinline__ void cell_insert(const PrepareParams& p, const JobDev& J,
+                                            uint64_t key, uint32_t win) {
+  const uint32_t mask = J.cell_cap - 1;
+  uint32_t h = slot_hash(key, mask);
+  for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
+    uint64_t* slot = p.ckeys + J.cell_off + h;
+    const uint64_t k = __ldcg((const unsigned long long*)slot);
+    bool mine = k == key;
+    if (!mine && k == kEmptyKey) {
+      const uint64_t old = atomicCAS((unsigned long long*)slot, kEmptyKey, key);
+      mine = old == kEmptyKey || old == key;
+    }
+    if (mine) {
+      atomicMin(p.cmin + J.cell_off + h, win);
+      atomicMax(p.cmax + J.cell_off + h, win);
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+}
+
+// True when the cell holds a deposit of a window other than `win`.
+__device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDev& J,
+                                             uint64_t key, uint32_t win) {
+  const uint32_t mask = J.cell_cap - 1;
+  uint32_t h = slot_hash(key, mask);
+  for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
+    const uint64_t k = __ldcg((const unsigned long long*)(p.ckeys + J.cell_off + h));
+    if (k == key) return __ldcg(p.cmin + J.cell_off + h) != win || __ldcg(p.cmax + J.cell_off + h) != win;
+    if (k == kEmptyKey) return false;
+    h = (h + 1) & mask;
+  }
+  return true;
+}
+
 __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
   const int64_t b = blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
@@ -196,6 +242,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       p.PDZ2[dst] = st_dmul(dz, dz);
       p.PV[dst] = __ddiv_rn(J.edep[i], J.denom);
       p.PKZ[dst] = (uint32_t)(long long)kd;
+      if (J.flagged) {
+        p.PZ[dst] = z1;
+        cell_insert(p, J, cell_key(x, y, z1, J.cell_size, 0, 0, 0), (uint32_t)(k / kWindow));
+      }
     }
     run += total;
     __syncthreads();
@@ -218,6 +268,31 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
   p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
   p.PV[dst] = 0.0;
   p.PKZ[dst] = 0;
+}
+
+// Boundary flags of the kept deposits of flagged jobs: a deposit is a boundary deposit when one of
+// the 27 cells around it holds a deposit of another window. A sphere whose hits in a window are
+// all non-boundary has no hit in any other window (its hits are within distance d of each other),
+// so the fused kernel can bin it as soon as the window is done.
+__global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
+  const int64_t b = blockIdx.x;
+  const int j = find_job(p.blk_prefix, p.n_jobs, b);
+  const JobDev J = p.jobs[j];
+  if (!J.flagged) return;
+  const int64_t k0 = p.blk_offset[b];
+  const int cnt = p.blk_count[b];
+  for (int q = threadIdx.x; q < cnt; q += kPrepThreads) {
+    const int64_t k = k0 + q;
+    const int64_t w = k / kWarpTile;
+    const int rem = (int)(k - w * kWarpTile);
+    const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+    const double x = p.PX[dst], y = p.PY[dst], z = p.PZ[dst];
+    const uint32_t win = (uint32_t)(k / kWindow);
+    bool boundary = false;
+    for (int c = 0; c < 27 && !boundary; ++c)
+      boundary = cell_foreign(p, J, cell_key(x, y, z, J.cell_size, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win);
+    if (boundary) p.PKZ[dst] |= kBoundaryBit;
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -267,12 +342,14 @@ struct SmemTable {
   unsigned long long* lo;
   unsigned long long* hi;
   uint16_t* used;
+  unsigned int* flags;   // CAP bits: the entry holds a boundary deposit's contribution
 };
 
 struct CtaState {
   int item;
   int tcount;
-  int spilled;
+  int spilled;      // some sphere of this oversample has a partial sum in the spill table
+  int overflow;     // this window sent a contribution to the spill table directly
   int edges_hist;   // histogram whose edges are in shared memory (-1: none)
 };
 
@@ -292,28 +369,32 @@ struct Spill {
 template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
                                            const FusedParams& P, const Spill& G, uint64_t key,
-                                           uint64_t lo, uint64_t hi) {
+                                           uint64_t lo, uint64_t hi, bool boundary) {
   constexpr int kHardLimit = (CAP * 3) / 4;
   if (*(volatile int*)&cs->tcount < kHardLimit) {
     uint32_t h = slot_hash(key, CAP - 1);
 #pragma unroll 1
     for (int probe = 0; probe < 32; ++probe) {
       const uint64_t k = ((volatile uint64_t*)T.keys)[h];
-      if (k == key) { acc_add(&T.lo[h], &T.hi[h], lo, hi); return; }
-      if (k == kEmptyKey) {
+      bool mine = k == key;
+      if (!mine && k == kEmptyKey) {
         const uint64_t old = atomicCAS((unsigned long long*)&T.keys[h], kEmptyKey, key);
         if (old == kEmptyKey) {
           const int idx = atomicAdd(&cs->tcount, 1);
           T.used[idx] = (uint16_t)h;
-          acc_add(&T.lo[h], &T.hi[h], lo, hi);
-          return;
         }
-        if (old == key) { acc_add(&T.lo[h], &T.hi[h], lo, hi); return; }
+        mine = old == kEmptyKey || old == key;
+      }
+      if (mine) {
+        acc_add(&T.lo[h], &T.hi[h], lo, hi);
+        if (boundary) atomicOr(&T.flags[h >> 5], 1u << (h & 31));
+        return;
       }
       h = (h + 1) & (CAP - 1);
     }
   }
   *(volatile int*)&cs->spilled = 1;
+  *(volatile int*)&cs->overflow = 1;
   if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, key, lo, hi))
     atomicOr(P.error_flags, 1);
 }
@@ -407,6 +488,7 @@ __device__ __forceinline__ void flush_to_spill(const SmemTable<CAP>& T, int cnt,
 template <int CAP, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   static_assert(CAP <= 65536, "used-slot list stores 16-bit slot indices");
+  static_assert(THREADS / 32 == kFusedWarps, "a window is one CTA tile of warp tiles");
   constexpr int kWarps = THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ CtaState cs;
@@ -420,6 +502,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   double* sedges = hyfy + HB;                                   // HB + 1 edges
   unsigned int* hcount = reinterpret_cast<unsigned int*>(sedges + HB + 1);
   T.used = reinterpret_cast<uint16_t*>(hcount + HB);
+  T.flags = reinterpret_cast<unsigned int*>(T.used + CAP);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -432,7 +515,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
 
   for (int i = tid; i < CAP; i += THREADS) { T.keys[i] = kEmptyKey; T.lo[i] = 0; T.hi[i] = 0; }
   for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
-  if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.edges_hist = -1; }
+  for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
+  if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; cs.edges_hist = -1; }
   __syncthreads();
 
   for (;;) {
@@ -529,21 +613,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
           inbox += __popc(boxmask);
           // runs of equal keys inside the lane's consecutive deposits are summed in registers
           uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
+          bool rflag = false;
 #pragma unroll
           for (int p = 0; p < kDepPerLane; ++p) {
             if (hitmask & (1u << p)) {
               const int64_t idx = tb + p * 32;
               const double v = __ldg(&P.PV[idx]);
-              const uint32_t kz = __ldg(&P.PKZ[idx]);
-              const uint64_t key =
-                  (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N + (uint64_t)kz * J.N2;
+              const uint32_t kzw = __ldg(&P.PKZ[idx]);
+              const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N +
+                                   (uint64_t)(kzw & ~kBoundaryBit) * J.N2;
+              const bool bflag = (kzw & kBoundaryBit) != 0;
               uint64_t lo, hi;
               to_fixed(v, E0, &lo, &hi);
               if (key == rkey) {
                 add128(rlo, rhi, lo, hi);
+                rflag |= bflag;
               } else {
-                if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi);
-                rkey = key; rlo = lo; rhi = hi;
+                if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
+                rkey = key; rlo = lo; rhi = hi; rflag = bflag;
               }
             }
           }
@@ -559,15 +646,44 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
               const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
               const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
               const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
+              const bool oflag = __shfl_up_sync(0xffffffffu, rflag, o);
               if (lane >= o && !head) {
                 add128(rlo, rhi, olo, ohi);
+                rflag |= oflag;
                 head = ohead;
               }
             }
-            if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi);
+            if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
           }
         }
-        if (wt0 + kWarps < n_wt) {
+        if (J.flagged) {
+          // window done: spheres without boundary contributions are complete -> bin them now;
+          // the others (or all, if the window overflowed) go to the spill table
+          __syncthreads();
+          const int cnt = cs.tcount;
+          const bool all_out = cs.overflow != 0;
+          int sent = 0;
+          for (int i = tid; i < cnt; i += THREADS) {
+            const uint32_t h = T.used[i];
+            const bool out = all_out || ((T.flags[h >> 5] >> (h & 31)) & 1u);
+            if (out) {
+              if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
+                atomicOr(P.error_flags, 1);
+              sent = 1;
+            } else {
+              bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
+            }
+            T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
+          }
+          sent = __syncthreads_or(sent);
+          for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
+          if (tid == 0) {
+            cs.tcount = 0;
+            cs.overflow = 0;
+            if (sent) cs.spilled = 1;
+          }
+          __syncthreads();
+        } else if (wt0 + kWarps < n_wt) {
           __syncthreads();
           if (cs.tcount > P.flush_threshold) {
             flush_to_spill<CAP, THREADS>(T, cs.tcount, P, G);
@@ -603,7 +719,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         }
       }
       __syncthreads();
-      if (tid == 0) { cs.tcount = 0; cs.spilled = 0; }
+      if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; }
       __syncthreads();
     }
 
@@ -667,19 +783,21 @@ constexpr int kFusedThreads = 512;
 // Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
 // 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
 // most kSmallHistBins bins.
-constexpr int kSmallHistBins = 768;
+constexpr int kSmallHistBins = 700;
 constexpr int kBigHistBins = 4096;
 
 size_t fused_smem_bytes(int cap, int hist_bins) {
-  return (size_t)cap * 26 + (size_t)hist_bins * 20 + 8;
+  return (size_t)cap * 26 + (size_t)cap / 8 + (size_t)hist_bins * 20 + 8;
 }
 
-cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, cudaStream_t s) {
+cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_flagged,
+                           cudaStream_t s) {
   if (n_blocks <= 0) return cudaSuccess;
   k_prep_count<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
   k_prep_scan<<<p.n_jobs, 1024, 0, s>>>(p);
   k_prep_write<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
   k_prep_pad<<<p.n_jobs, kWarpTile, 0, s>>>(p);
+  if (any_flagged) k_prep_flag<<<(unsigned)n_blocks, kPrepThreads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

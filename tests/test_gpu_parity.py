@@ -113,3 +113,21 @@ def test_no_shift_oversamples_repeat(ctx):
     w1.shift_track = False
     c1, _, s1, _ = gpu_run(ctx, w1)
     assert np.array_equal(gc[0], 5 * c1[0])
+
+
+@pytest.mark.parametrize("gen,d,n,n_os", [("ion", 2.0, 120_000, 4), ("ion", 10.0, 200_000, 5),
+                                          ("proton", 2.0, 60_000, 6), ("ion4", 10.0, 150_000, 4)])
+def test_window_boundary_flags(ctx, gen, d, n, n_os):
+    """Multi-window jobs on fine lattices (the prepare stage flags boundary deposits and the fused
+    kernel bins complete spheres per window): bit-exact with the oracle."""
+    if gen == "proton":
+        w = W.config0(n_tracks=1, n_dep=n, n_os=n_os)
+    elif gen == "ion4":
+        w = W.config4(n_tracks=1, n_dep=n, n_os=n_os)
+    else:
+        w = W.config1(n_tracks=1, n_dep=n, n_os=n_os)
+    w.diameter[:] = d
+    gc, gy, gs, _ = gpu_run(ctx, w)
+    oc, oy, os_, _ = oracle_run(w)
+    assert_stats_equal(gs, os_)
+    assert_hist_equal(gc, gy, oc, oy)
