@@ -107,7 +107,7 @@ struct st_ctx {
   float t_prep = 0, t_fused = 0;
   int32_t launches = 0;
 
-  int64_t item_cost = 1 << 20;
+  int64_t item_cost = 1 << 18;
   int grid_override = 0;
   int smem_hist_bins = 4096;
   bool fused_configured = false;
