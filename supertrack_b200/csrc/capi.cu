@@ -19,6 +19,7 @@ cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_fl
 cudaError_t configure_fused();
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
+cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
 }  // namespace st
 
 namespace {
@@ -93,6 +94,8 @@ struct st_ctx {
   DevBuf px, py, pdz2, pv, pkz;
   DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off;
   DevBuf c_keys, c_min, c_max, pz;   // cell arena and shifted z of flagged jobs
+  DevBuf u_next, u_done, u_table, pool;  // shared units and the spill-table pool
+  DevBuf d_plan, d_plan_misc;             // planner: per-job plans and scratch counters
   DevBuf g_keys, g_lo, g_hi, g_used, g_count;
   uint32_t gcap = 0;
   int ggrid = 0;
@@ -124,6 +127,11 @@ struct st_ctx {
   int cache_max_nbins = 0;
   int64_t cache_cells = 0;
   bool cache_any_flagged = false;
+  int64_t cache_units = 0;
+  int64_t cache_item_cap = 0;
+  st::PlanParams cache_plan{};
+  int chunk_windows = 4;      // windows (4096 deposits each) per chunk of a shared unit
+  int max_helpers = 32;       // helper items per shared unit
 };
 
 namespace {
@@ -290,31 +298,27 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     max_nbins = std::max(max_nbins, c->hists[c->jobs[first + i].desc.hist_id].nbins);
   c->cache_max_nbins = max_nbins;
 
-  // work items: oversample blocks of roughly item_cost deposit*oversamples, longest first
-  std::vector<WorkItem> items;
+  // work items are planned on the device from the kept counts (k_plan_*); here only their
+  // capacity: every job as shared units with the most helpers is the upper bound
+  int64_t total_os = 0, work_jobs = 0;
   for (size_t i = 0; i < nj; ++i) {
     const JobHost& J = c->jobs[first + i];
-    const int64_t nos = J.desc.n_oversamples;
-    if (nos == 0 || J.track.n == 0) continue;
-    int64_t blk_os = std::max<int64_t>(1, c->item_cost / J.n_pad);
-    blk_os = std::min<int64_t>(blk_os, nos);
-    for (int64_t o = 0; o < nos; o += blk_os) {
-      WorkItem w;
-      w.job = (int32_t)i;
-      w.os_begin = (int32_t)o;
-      w.os_count = (int32_t)std::min<int64_t>(blk_os, nos - o);
-      w.pad = 0;
-      items.push_back(w);
-    }
+    if (J.desc.n_oversamples == 0 || J.track.n == 0) continue;
+    total_os += J.desc.n_oversamples;
+    ++work_jobs;
   }
-  std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
-    return jd[a.job].n_pad * a.os_count > jd[b.job].n_pad * b.os_count;
-  });
+  const int64_t item_cap = std::max<int64_t>(1, total_os * std::max(1, c->max_helpers));
+  const int64_t units = std::max<int64_t>(1, total_os);
+  ST_CUDA(ensure(c->u_next, (size_t)units * 4), "units");
+  ST_CUDA(ensure(c->u_done, (size_t)units * 4), "units");
+  ST_CUDA(ensure(c->u_table, (size_t)units * 4), "units");
+  ST_CUDA(ensure(c->d_items, (size_t)item_cap * sizeof(WorkItem)), "items");
+  ST_CUDA(ensure(c->d_plan, nj * sizeof(st::JobPlan)), "plan");
+  ST_CUDA(ensure(c->d_plan_misc, 4096), "plan scratch");
 
   ST_CUDA(ensure(c->d_jobs, nj * sizeof(JobDev)), "job table");
   ST_CUDA(ensure(c->d_aux, nj * sizeof(JobAux)), "job aux");
   ST_CUDA(ensure(c->d_hists, std::max<size_t>(1, hd.size()) * sizeof(HistDev)), "hist table");
-  ST_CUDA(ensure(c->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)), "items");
   ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
   ST_CUDA(ensure(c->d_blk_count, (size_t)blk[nj] * 4), "prepare block counts");
   ST_CUDA(ensure(c->c_keys, (size_t)cells_total * 8), "cell arena");
@@ -327,14 +331,12 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, jd.data(), nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
   if (!hd.empty())
     ST_CUDA(cudaMemcpyAsync(c->d_hists.p, hd.data(), hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
-  if (!items.empty())
-    ST_CUDA(cudaMemcpyAsync(c->d_items.p, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, c->stream), "upload items");
   ST_CUDA(cudaMemcpyAsync(c->d_blk.p, blk.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
 
   // spill tables: one per resident CTA, able to hold every distinct sphere of the largest job;
   // the number of resident CTAs shrinks if the tables would exceed 30% of free memory
   int grid = c->grid_override > 0 ? c->grid_override : c->sm_count;
-  grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)items.size()));
+  grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, work_jobs * std::max(1, c->max_helpers)));
   const uint32_t gcap = std::max(c->gcap, next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024)));
   {
     size_t free_b = 0, total_b = 0;
@@ -348,6 +350,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     st_status s = init_spill_tables(c, gcap, grid);
     if (s != ST_OK) return s;
   }
+  ST_CUDA(ensure(c->pool, (size_t)((grid + 31) / 32) * 4), "spill-table pool");
   if (!c->fused_configured) {
     ST_CUDA(st::configure_fused(), "configure fused kernel");
     c->fused_configured = true;
@@ -375,7 +378,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   fp.aux = pp.aux;
   fp.hists = (const HistDev*)c->d_hists.p;
   fp.items = (const WorkItem*)c->d_items.p;
-  fp.n_items = (int32_t)items.size();
+  fp.n_items = (const int*)((char*)c->d_plan_misc.p + 8);
   fp.flush_threshold = 1024;
   fp.work_counter = (unsigned int*)c->d_counter.p;
   fp.PX = pp.PX; fp.PY = pp.PY; fp.PDZ2 = pp.PDZ2; fp.PV = pp.PV; fp.PKZ = pp.PKZ;
@@ -390,13 +393,41 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   fp.export_count = nullptr;
   fp.export_cap = 0;
   fp.error_flags = (int*)c->d_err.p;
+  fp.unit_next = (unsigned int*)c->u_next.p;
+  fp.unit_done = (unsigned int*)c->u_done.p;
+  fp.unit_table = (int*)c->u_table.p;
+  fp.pool_bits = (unsigned int*)c->pool.p;
+  fp.chunk_windows = c->chunk_windows;
+  fp.pad2 = 0;
 
   c->cache_aux = std::move(aux);
   c->cache_blocks = blk[nj];
-  c->cache_grid = items.empty() ? 0 : grid;
+  c->cache_grid = work_jobs == 0 ? 0 : grid;
+  c->cache_item_cap = item_cap;
   c->cache_arena_total = arena_total;
   c->cache_cells = cells_total;
   c->cache_any_flagged = any_flagged;
+  c->cache_units = units;
+  // planner parameters; the scratch block holds total_units (8 B), n_items (4 B), the unit
+  // counter (4 B) and the three bucket arrays
+  st::PlanParams& q = c->cache_plan;
+  char* m = (char*)c->d_plan_misc.p;
+  q.jobs = (const JobDev*)c->d_jobs.p;
+  q.aux = (const JobAux*)c->d_aux.p;
+  q.n_jobs = (int32_t)nj;
+  q.chunk_windows = c->chunk_windows;
+  q.max_helpers = c->max_helpers;
+  q.grid = std::max(1, grid);
+  q.item_cost = c->item_cost;
+  q.total_units = (unsigned long long*)m;
+  q.n_items = (int*)(m + 8);
+  q.unit_counter = (unsigned int*)(m + 12);
+  q.bucket_count = (unsigned int*)(m + 16);
+  q.bucket_start = q.bucket_count + st::kPlanBuckets;
+  q.bucket_cursor = q.bucket_start + st::kPlanBuckets;
+  q.plan = (st::JobPlan*)c->d_plan.p;
+  q.items = (WorkItem*)c->d_items.p;
+  q.item_cap = item_cap;
   c->cache_first = first;
   c->cache_last = last;
   c->cache_valid = !want_export;
@@ -422,6 +453,14 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   }
   ST_CUDA(cudaMemcpyAsync(c->d_aux.p, c->cache_aux.data(), nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
   ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
+  if (c->cache_grid > 0)
+    ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
+  ST_CUDA(cudaMemsetAsync(c->d_plan_misc.p, 0, 16 + 3 * 4 * st::kPlanBuckets, c->stream), "plan reset");
+  if (c->cache_units > 0) {
+    ST_CUDA(cudaMemsetAsync(c->u_next.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+    ST_CUDA(cudaMemsetAsync(c->u_done.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+    ST_CUDA(cudaMemsetAsync(c->u_table.p, 0xFF, (size_t)c->cache_units * 4, c->stream), "unit reset");
+  }
   if (c->cache_cells > 0) {
     ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
     ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
@@ -441,6 +480,7 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
 
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
   ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->cache_any_flagged, c->stream), "prepare launch");
+  ST_CUDA(st::launch_plan(c->cache_plan, c->stream), "plan launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
   ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->stream), "fused launch");
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
@@ -623,7 +663,8 @@ st_status st_ctx_destroy(st_ctx* c) {
   DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pv, &c->pkz,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
                     &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->c_keys,
-                    &c->c_min, &c->c_max, &c->pz, &c->g_keys, &c->g_lo, &c->g_hi,
+                    &c->c_min, &c->c_max, &c->pz, &c->u_next, &c->u_done, &c->u_table,
+                    &c->pool, &c->d_plan, &c->d_plan_misc, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};
   for (DevBuf* b : bufs) release(*b);

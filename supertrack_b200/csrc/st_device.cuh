@@ -90,7 +90,8 @@ struct WorkItem {
   int32_t job;
   int32_t os_begin;
   int32_t os_count;
-  int32_t pad;
+  int32_t unit;       // -1: the CTA does every window of os_begin..+os_count; else a helper of
+                      // shared unit `unit` (one oversample of a large job, split into chunks)
 };
 
 // One exported sphere: (oversample, key, lineal energy, hit deposits).
@@ -106,7 +107,7 @@ struct FusedParams {
   JobAux* aux;
   const HistDev* hists;
   const WorkItem* items;
-  int32_t n_items;
+  const int* n_items;         // written by the planner
   int32_t flush_threshold;    // smem table occupancy that triggers a flush to the spill table
   unsigned int* work_counter; // next item to claim
   const double* PX;
@@ -126,7 +127,15 @@ struct FusedParams {
   SphereRecord* export_buf;
   unsigned long long* export_count;
   unsigned long long export_cap;
-  int* error_flags;           // bit 0: spill table full, bit 1: export buffer full
+  int* error_flags;           // bit 0: spill table full, bit 1: export buffer full,
+                              // bit 2: spill-table pool exhausted, bit 3: unit wait gave up
+  // shared units (one oversample of a large job, processed in chunks by several CTAs)
+  unsigned int* unit_next;    // next chunk to claim
+  unsigned int* unit_done;    // chunks finished
+  int* unit_table;            // spill table of the unit (-1 none yet, -2 being acquired)
+  unsigned int* pool_bits;    // spill tables in use (one bit per table, gridDim.x tables)
+  int32_t chunk_windows;      // windows per chunk
+  int32_t pad2;
 };
 
 struct PrepareParams {
@@ -145,6 +154,33 @@ struct PrepareParams {
   double* PDZ2;
   double* PV;
   uint32_t* PKZ;
+};
+
+// Device-side planning of the fused kernel's work items from the kept deposit counts.
+constexpr int kPlanBuckets = 64;
+struct JobPlan {
+  int32_t items;
+  int32_t bucket;
+  int32_t unit_base;   // -1: private items
+  int32_t blk_os;      // oversamples per private item, or helpers per unit
+};
+struct PlanParams {
+  const JobDev* jobs;
+  const JobAux* aux;
+  int32_t n_jobs;
+  int32_t chunk_windows;
+  int32_t max_helpers;
+  int32_t grid;
+  long long item_cost;
+  unsigned long long* total_units;   // sum of kept * n_os
+  unsigned int* bucket_count;        // kPlanBuckets
+  unsigned int* bucket_start;        // kPlanBuckets
+  unsigned int* bucket_cursor;       // kPlanBuckets
+  unsigned int* unit_counter;
+  JobPlan* plan;
+  WorkItem* items;
+  int* n_items;
+  long long item_cap;
 };
 
 constexpr int kPrepThreads = 256;

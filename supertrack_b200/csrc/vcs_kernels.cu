@@ -483,15 +483,240 @@ __device__ __forceinline__ void flush_to_spill(const SmemTable<CAP>& T, int cnt,
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_fused
+// Spill-table pool: one table per CTA of the launch. A CTA holds at most one table at a time
+// (for its private item, or for the shared unit it works on until the unit is binned), so a free
+// table always exists; the bounded scan only guards against a logic error.
+// ---------------------------------------------------------------------------------------------
+__device__ int pool_acquire(unsigned int* bits, int n_tables, int* err) {
+  const int words = (n_tables + 31) / 32;
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    for (int w = 0; w < words; ++w) {
+      const unsigned valid = (w == words - 1 && (n_tables & 31)) ? ((1u << (n_tables & 31)) - 1u) : ~0u;
+      unsigned freeb = ~__ldcg(&bits[w]) & valid;
+      while (freeb) {
+        const int b = __ffs(freeb) - 1;
+        const unsigned old = atomicOr(&bits[w], 1u << b);
+        if (!(old & (1u << b))) return w * 32 + b;
+        freeb &= ~(1u << b);
+      }
+    }
+  }
+  atomicOr(err, 4);
+  return -1;
+}
+
+__device__ __forceinline__ void pool_release(unsigned int* bits, int t) {
+  atomicAnd(&bits[t >> 5], ~(1u << (t & 31)));
+}
+
+// Table of shared unit u: the first helper acquires it, the others wait (bounded) until it is
+// published.
+__device__ int unit_table_get(const FusedParams& P, int u) {
+  int t = atomicCAS(&P.unit_table[u], -1, -2);
+  if (t == -1) {
+    t = pool_acquire(P.pool_bits, gridDim.x, P.error_flags);
+    atomicExch(&P.unit_table[u], t < 0 ? -3 : t);
+    return t;
+  }
+  for (long long spin = 0; t == -2 && spin < (1ll << 24); ++spin) {
+    __nanosleep(64);
+    t = *(volatile int*)&P.unit_table[u];
+  }
+  if (t < 0) { atomicOr(P.error_flags, 8); return -1; }
+  return t;
+}
+
+__device__ __forceinline__ Spill spill_of(const FusedParams& P, int t, long long kept) {
+  Spill G;
+  G.keys = P.gkeys + (size_t)t * P.gcap;
+  G.lo = P.glo + (size_t)t * P.gcap;
+  G.hi = P.ghi + (size_t)t * P.gcap;
+  G.used = P.gused + (size_t)t * P.gcap;
+  G.count = P.gcount + t;
+  uint32_t cap = 1024;
+  while (cap < P.gcap && (long long)cap < 2 * kept) cap <<= 1;
+  G.cap = cap;
+  return G;
+}
+
+// Bins and clears every entry of a spill table (all threads of the CTA).
+template <int THREADS>
+__device__ __forceinline__ void bin_spill(const Spill& G, const BinContext& B, const FusedParams& P,
+                                          unsigned long long& spheres, unsigned long long& binned) {
+  const unsigned gc = __ldcg(G.count);
+  for (unsigned i = threadIdx.x; i < gc; i += THREADS) {
+    const uint32_t h = __ldcg(&G.used[i]);
+    const uint64_t key = __ldcg((const unsigned long long*)&G.keys[h]);
+    const uint64_t lo = __ldcg(&G.lo[h]);
+    const uint64_t hi = __ldcg(&G.hi[h]);
+    bin_sphere(B, P, key, lo, hi, spheres, binned);
+    G.keys[h] = kEmptyKey; G.lo[h] = 0; G.hi[h] = 0;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *G.count = 0;
+    __threadfence();
+  }
+}
+
+struct FusedJob {
+  JobDev J;
+  int E0;
+  int64_t n_wt;     // warp tiles of kept deposits
+};
+
+// Superimposes oversample `os` of a job over warp tiles [wt_begin, wt_end) (whole windows):
+// shift, box test, lattice test, key, exact run / warp / shared-memory reduction. For flagged jobs
+// every window ends by binning its complete spheres and moving boundary spheres to G; otherwise
+// spheres accumulate across windows and the shared table spills to G when it fills up.
+template <int CAP, int THREADS>
+__device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob& F,
+                                            const SmemTable<CAP>& T, CtaState& cs,
+                                            const Spill& G, const BinContext& B, int os,
+                                            int64_t wt_begin, int64_t wt_end,
+                                            unsigned long long& hits, unsigned long long& inbox,
+                                            unsigned long long& spheres,
+                                            unsigned long long& binned) {
+  constexpr int kWarps = THREADS / 32;
+  const JobDev& J = F.J;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float ux, uy;
+  shift_uniforms(J.seed, J.track_id, (uint32_t)os, J.shift_track, &ux, &uy);
+  const double sx = shift_from_uniform(ux, J.L, J.HL);
+  const double sy = shift_from_uniform(uy, J.L, J.HL);
+
+  for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps) {
+    const int64_t w = wt0 + warp;
+    if (w < wt_end) {
+      const int64_t tb = J.prep_off + w * kWarpTile + lane;
+      double xv[kDepPerLane], yv[kDepPerLane];
+#pragma unroll
+      for (int p = 0; p < kDepPerLane; ++p) {
+        xv[p] = __ldg(&P.PX[tb + p * 32]);
+        yv[p] = __ldg(&P.PY[tb + p * 32]);
+      }
+      uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
+      unsigned hitmask = 0, boxmask = 0;
+#pragma unroll
+      for (int p = 0; p < kDepPerLane; ++p) {
+        const double x1 = st_dadd(xv[p], sx);
+        const double y1 = st_dadd(yv[p], sy);
+        kxv[p] = 0;
+        kyv[p] = 0;
+        if (fabs(x1) < J.HL && fabs(y1) < J.HL) {
+          boxmask |= 1u << p;
+          const double dz2 = __ldg(&P.PDZ2[tb + p * 32]);
+          const double ax = st_dsub(x1, J.gSO);
+          const double ay = st_dsub(y1, J.gSO);
+          double kdx, kdy;
+          lattice_index(ax, J.d, J.inv_d, kxv[p], kdx);
+          lattice_index(ay, J.d, J.inv_d, kyv[p], kdy);
+          const double ddx = st_dsub(st_dmul(kdx, J.d), ax);
+          const double ddy = st_dsub(st_dmul(kdy, J.d), ay);
+          const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dz2);
+          if (dist <= J.r2) hitmask |= 1u << p;
+        }
+      }
+      hits += __popc(hitmask);
+      inbox += __popc(boxmask);
+      // runs of equal keys inside the lane's consecutive deposits are summed in registers
+      uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
+      bool rflag = false;
+#pragma unroll
+      for (int p = 0; p < kDepPerLane; ++p) {
+        if (hitmask & (1u << p)) {
+          const int64_t idx = tb + p * 32;
+          const double v = __ldg(&P.PV[idx]);
+          const uint32_t kzw = __ldg(&P.PKZ[idx]);
+          const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N +
+                               (uint64_t)(kzw & ~kBoundaryBit) * J.N2;
+          const bool bflag = (kzw & kBoundaryBit) != 0;
+          uint64_t lo, hi;
+          to_fixed(v, F.E0, &lo, &hi);
+          if (key == rkey) {
+            add128(rlo, rhi, lo, hi);
+            rflag |= bflag;
+          } else {
+            if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
+            rkey = key; rlo = lo; rhi = hi; rflag = bflag;
+          }
+        }
+      }
+      // the lanes' last runs: segmented sum over consecutive lanes with the same key, so a
+      // sphere spanning several lanes costs one shared-memory update
+      {
+        const uint64_t kprev = __shfl_up_sync(0xffffffffu, rkey, 1);
+        const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
+        bool head = lane == 0 || kprev != rkey;
+        const bool tail = lane == 31 || knext != rkey;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
+          const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
+          const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
+          const bool oflag = __shfl_up_sync(0xffffffffu, rflag, o);
+          if (lane >= o && !head) {
+            add128(rlo, rhi, olo, ohi);
+            rflag |= oflag;
+            head = ohead;
+          }
+        }
+        if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
+      }
+    }
+    if (J.flagged) {
+      // window done: spheres without boundary contributions are complete -> bin them now;
+      // the others (or all, if the window overflowed) go to the spill table
+      __syncthreads();
+      const int cnt = cs.tcount;
+      const bool all_out = cs.overflow != 0;
+      int sent = 0;
+      for (int i = tid; i < cnt; i += THREADS) {
+        const uint32_t h = T.used[i];
+        const bool out = all_out || ((T.flags[h >> 5] >> (h & 31)) & 1u);
+        if (out) {
+          if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
+            atomicOr(P.error_flags, 1);
+          sent = 1;
+        } else {
+          bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
+        }
+        T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
+      }
+      sent = __syncthreads_or(sent);
+      for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
+      if (tid == 0) {
+        cs.tcount = 0;
+        cs.overflow = 0;
+        if (sent) cs.spilled = 1;
+      }
+      __syncthreads();
+    } else if (wt0 + kWarps < wt_end) {
+      __syncthreads();
+      if (cs.tcount > P.flush_threshold) {
+        flush_to_spill<CAP, THREADS>(T, cs.tcount, P, G);
+        __syncthreads();
+        if (tid == 0) { cs.tcount = 0; cs.spilled = 1; }
+        __syncthreads();
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_fused: persistent work-stealing kernel. Items are either private (every window of a block of
+// oversamples of a small or medium job, one CTA) or helpers of a shared unit (one oversample of
+// a large job, whose window chunks are claimed dynamically by every helper that arrives).
 // ---------------------------------------------------------------------------------------------
 template <int CAP, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   static_assert(CAP <= 65536, "used-slot list stores 16-bit slot indices");
   static_assert(THREADS / 32 == kFusedWarps, "a window is one CTA tile of warp tiles");
-  constexpr int kWarps = THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ CtaState cs;
+  __shared__ int s_bcast[2];
 
   const int HB = P.smem_hist_bins;
   SmemTable<CAP> T;
@@ -506,12 +731,6 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const int warp = tid >> 5;
-  uint64_t* gk_base = P.gkeys + (size_t)blockIdx.x * P.gcap;
-  unsigned long long* glo_base = P.glo + (size_t)blockIdx.x * P.gcap;
-  unsigned long long* ghi_base = P.ghi + (size_t)blockIdx.x * P.gcap;
-  uint32_t* gused_base = P.gused + (size_t)blockIdx.x * P.gcap;
-  unsigned int* gcnt = P.gcount + blockIdx.x;
 
   for (int i = tid; i < CAP; i += THREADS) { T.keys[i] = kEmptyKey; T.lo[i] = 0; T.hi[i] = 0; }
   for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
@@ -525,21 +744,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     const int it = cs.item;
     const int cached_hist = cs.edges_hist;
     __syncthreads();
-    if (it >= P.n_items) break;
+    if (it >= *P.n_items) break;
 
     const WorkItem W = P.items[it];
-    const JobDev J = P.jobs[W.job];
     const JobAux A = P.aux[W.job];
     if (A.flags & kAuxNonfinite) continue;  // rejected job: contributes nothing, host reports it
-    const HistDev H = P.hists[J.hist];
-    const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
+    FusedJob F;
+    F.J = P.jobs[W.job];
+    F.E0 = choose_grid_exponent(A.e_min, A.e_max, F.J.n, A.flags & kAuxNonzero);
+    F.n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
+    const HistDev H = P.hists[F.J.hist];
     const bool smem_hist = H.nbins <= HB;
 
     // histogram edges into shared memory (kept while consecutive items use the same histogram)
-    if (smem_hist && cached_hist != J.hist) {
+    if (smem_hist && cached_hist != F.J.hist) {
       for (int i = tid; i <= H.nbins; i += THREADS) sedges[i] = H.edges[i];
       __syncthreads();
-      if (tid == 0) cs.edges_hist = J.hist;
+      if (tid == 0) cs.edges_hist = F.J.hist;
     }
 
     BinContext B;
@@ -550,185 +771,98 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     B.mode = H.mode;
     B.ca = H.ca;
     B.cb = H.cb;
-    B.E0 = E0;
+    B.E0 = F.E0;
     B.job = W.job;
     B.hcount = smem_hist ? hcount : nullptr;
     B.hyfy = smem_hist ? hyfy : nullptr;
 
-    Spill G;
-    G.keys = gk_base;
-    G.lo = glo_base;
-    G.hi = ghi_base;
-    G.used = gused_base;
-    G.count = gcnt;
-    {
-      uint32_t cap = 1024;
-      while (cap < P.gcap && (long long)cap < 2 * A.kept) cap <<= 1;
-      G.cap = cap;
-    }
-
-    const int64_t n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
     unsigned long long hits = 0, spheres = 0, binned = 0, inbox = 0;
 
-    for (int os = W.os_begin; os < W.os_begin + W.os_count; ++os) {
-      float ux, uy;
-      shift_uniforms(J.seed, J.track_id, (uint32_t)os, J.shift_track, &ux, &uy);
-      const double sx = shift_from_uniform(ux, J.L, J.HL);
-      const double sy = shift_from_uniform(uy, J.L, J.HL);
-      B.os = os;
-
-      for (int64_t wt0 = 0; wt0 < n_wt; wt0 += kWarps) {
-        const int64_t w = wt0 + warp;
-        if (w < n_wt) {
-          const int64_t tb = J.prep_off + w * kWarpTile + lane;
-          double xv[kDepPerLane], yv[kDepPerLane], dv[kDepPerLane];
-#pragma unroll
-          for (int p = 0; p < kDepPerLane; ++p) {
-            xv[p] = __ldg(&P.PX[tb + p * 32]);
-            yv[p] = __ldg(&P.PY[tb + p * 32]);
-            dv[p] = __ldg(&P.PDZ2[tb + p * 32]);
-          }
-          uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
-          unsigned hitmask = 0, boxmask = 0;
-#pragma unroll
-          for (int p = 0; p < kDepPerLane; ++p) {
-            const double x1 = st_dadd(xv[p], sx);
-            const double y1 = st_dadd(yv[p], sy);
-            kxv[p] = 0;
-            kyv[p] = 0;
-            if (fabs(x1) < J.HL && fabs(y1) < J.HL) {
-              boxmask |= 1u << p;
-              const double ax = st_dsub(x1, J.gSO);
-              const double ay = st_dsub(y1, J.gSO);
-              double kdx, kdy;
-              lattice_index(ax, J.d, J.inv_d, kxv[p], kdx);
-              lattice_index(ay, J.d, J.inv_d, kyv[p], kdy);
-              const double ddx = st_dsub(st_dmul(kdx, J.d), ax);
-              const double ddy = st_dsub(st_dmul(kdy, J.d), ay);
-              const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dv[p]);
-              if (dist <= J.r2) hitmask |= 1u << p;
-            }
-          }
-          hits += __popc(hitmask);
-          inbox += __popc(boxmask);
-          // runs of equal keys inside the lane's consecutive deposits are summed in registers
-          uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
-          bool rflag = false;
-#pragma unroll
-          for (int p = 0; p < kDepPerLane; ++p) {
-            if (hitmask & (1u << p)) {
-              const int64_t idx = tb + p * 32;
-              const double v = __ldg(&P.PV[idx]);
-              const uint32_t kzw = __ldg(&P.PKZ[idx]);
-              const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N +
-                                   (uint64_t)(kzw & ~kBoundaryBit) * J.N2;
-              const bool bflag = (kzw & kBoundaryBit) != 0;
-              uint64_t lo, hi;
-              to_fixed(v, E0, &lo, &hi);
-              if (key == rkey) {
-                add128(rlo, rhi, lo, hi);
-                rflag |= bflag;
-              } else {
-                if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
-                rkey = key; rlo = lo; rhi = hi; rflag = bflag;
-              }
-            }
-          }
-          // the lanes' last runs: segmented sum over consecutive lanes with the same key, so a
-          // sphere spanning several lanes costs one shared-memory update
-          {
-            const uint64_t kprev = __shfl_up_sync(0xffffffffu, rkey, 1);
-            const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
-            bool head = lane == 0 || kprev != rkey;
-            const bool tail = lane == 31 || knext != rkey;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-              const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
-              const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
-              const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
-              const bool oflag = __shfl_up_sync(0xffffffffu, rflag, o);
-              if (lane >= o && !head) {
-                add128(rlo, rhi, olo, ohi);
-                rflag |= oflag;
-                head = ohead;
-              }
-            }
-            if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
-          }
+    // Segments: a private item walks its oversamples (all windows each) with one pool table; a
+    // helper claims window chunks of its shared unit until none is left.
+    const bool shared = W.unit >= 0;
+    const int64_t wpc = (int64_t)P.chunk_windows * kFusedWarps;  // warp tiles per chunk
+    const int64_t n_chunks = (F.n_wt + wpc - 1) / wpc;
+    int private_table = -1;
+    if (!shared) {
+      if (tid == 0) s_bcast[0] = pool_acquire(P.pool_bits, gridDim.x, P.error_flags);
+      __syncthreads();
+      private_table = s_bcast[0];
+      __syncthreads();
+    }
+    for (int seg = 0;; ++seg) {
+      int os, t;
+      int64_t wb, we;
+      if (!shared) {
+        if (private_table < 0 || seg >= W.os_count) break;
+        os = W.os_begin + seg;
+        t = private_table;
+        wb = 0;
+        we = F.n_wt;
+      } else {
+        if (tid == 0) {
+          const unsigned c = atomicAdd(&P.unit_next[W.unit], 1u);
+          s_bcast[0] = (int64_t)c < n_chunks ? (int)c : -1;
+          s_bcast[1] = s_bcast[0] >= 0 ? unit_table_get(P, W.unit) : -1;
         }
-        if (J.flagged) {
-          // window done: spheres without boundary contributions are complete -> bin them now;
-          // the others (or all, if the window overflowed) go to the spill table
-          __syncthreads();
-          const int cnt = cs.tcount;
-          const bool all_out = cs.overflow != 0;
-          int sent = 0;
+        __syncthreads();
+        const int c = s_bcast[0];
+        t = s_bcast[1];
+        __syncthreads();
+        if (c < 0 || t < 0) break;
+        os = W.os_begin;
+        wb = (int64_t)c * wpc;
+        we = wb + wpc < F.n_wt ? wb + wpc : F.n_wt;
+      }
+      B.os = os;
+      const Spill G = spill_of(P, t, A.kept);
+      superimpose<CAP, THREADS>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
+      const int cnt = cs.tcount;
+      bool bin_table;
+      if (!shared) {
+        bin_table = cs.spilled != 0;
+        if (bin_table) {
+          flush_to_spill<CAP, THREADS>(T, cnt, P, G);
+        } else {
           for (int i = tid; i < cnt; i += THREADS) {
             const uint32_t h = T.used[i];
-            const bool out = all_out || ((T.flags[h >> 5] >> (h & 31)) & 1u);
-            if (out) {
-              if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
-                atomicOr(P.error_flags, 1);
-              sent = 1;
-            } else {
-              bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
-            }
+            bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
             T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
           }
-          sent = __syncthreads_or(sent);
-          for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
-          if (tid == 0) {
-            cs.tcount = 0;
-            cs.overflow = 0;
-            if (sent) cs.spilled = 1;
-          }
-          __syncthreads();
-        } else if (wt0 + kWarps < n_wt) {
-          __syncthreads();
-          if (cs.tcount > P.flush_threshold) {
-            flush_to_spill<CAP, THREADS>(T, cs.tcount, P, G);
-            __syncthreads();
-            if (tid == 0) { cs.tcount = 0; cs.spilled = 1; }
-            __syncthreads();
-          }
-        }
-      }
-      __syncthreads();
-
-      // ---- reduce-by-key complete for this oversample: bin every sphere
-      const int cnt = cs.tcount;
-      if (cs.spilled) {
-        flush_to_spill<CAP, THREADS>(T, cnt, P, G);
-        __syncthreads();
-        const unsigned gc = __ldcg(G.count);
-        for (unsigned i = tid; i < gc; i += THREADS) {
-          const uint32_t h = __ldcg(&G.used[i]);
-          const uint64_t key = __ldcg((const unsigned long long*)&G.keys[h]);
-          const uint64_t lo = __ldcg(&G.lo[h]);
-          const uint64_t hi = __ldcg(&G.hi[h]);
-          bin_sphere(B, P, key, lo, hi, spheres, binned);
-          G.keys[h] = kEmptyKey; G.lo[h] = 0; G.hi[h] = 0;
         }
         __syncthreads();
-        if (tid == 0) *G.count = 0;
       } else {
-        for (int i = tid; i < cnt; i += THREADS) {
-          const uint32_t h = T.used[i];
-          bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
-          T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
+        // everything left in shared memory may meet contributions of other chunks
+        flush_to_spill<CAP, THREADS>(T, cnt, P, G);
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+          const unsigned done = atomicAdd(&P.unit_done[W.unit], 1u) + 1u;
+          s_bcast[0] = (int64_t)done == n_chunks ? 1 : 0;
         }
+        __syncthreads();
+        bin_table = s_bcast[0] != 0;  // last chunk of the unit: every contribution is in G
+        if (bin_table) __threadfence();
       }
-      __syncthreads();
+      if (bin_table) {
+        bin_spill<THREADS>(G, B, P, spheres, binned);
+        if (shared && tid == 0) pool_release(P.pool_bits, t);
+      }
       if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; }
       __syncthreads();
+    }
+    if (private_table >= 0) {
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) pool_release(P.pool_bits, private_table);
     }
 
     // ---- per-item flush of the shared-memory histogram and the job statistics
     if (smem_hist) {
       for (int b = tid; b < H.nbins; b += THREADS) {
-        const unsigned c = hcount[b];
-        if (c) {
-          atomicAdd(&H.counts[b], (unsigned long long)c);
+        const unsigned cnt = hcount[b];
+        if (cnt) {
+          atomicAdd(&H.counts[b], (unsigned long long)cnt);
           atomicAdd(&H.yfy[b], hyfy[b]);
           hcount[b] = 0;
           hyfy[b] = 0.0;
@@ -750,6 +884,110 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     }
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Planner (after the prepare stage, before k_fused): work items from the kept deposit counts.
+// A job whose kept deposits per oversample exceed both four chunks and an eighth of one CTA's
+// share of the batch runs as shared units (one per oversample, `helpers` helper items each);
+// every other job runs as private items of about item_cost deposit*oversamples. Items are
+// bucketed by cost, largest first (longest-processing-time order at bucket granularity).
+// ---------------------------------------------------------------------------------------------
+__global__ void k_plan_total(PlanParams q) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long v = 0;
+  if (j < q.n_jobs) v = (unsigned long long)q.aux[j].kept * (unsigned long long)q.jobs[j].n_os;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(q.total_units, v);
+}
+
+__device__ __forceinline__ int cost_bucket(long long cost) {
+  int l = 0;
+  while (cost > 1 && l < 62) { cost >>= 1; ++l; }
+  return kPlanBuckets - 1 - l;  // larger cost -> smaller bucket -> earlier
+}
+
+__global__ void k_plan_size(PlanParams q) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= q.n_jobs) return;
+  const long long kept = q.aux[j].kept;
+  const long long nos = q.jobs[j].n_os;
+  JobPlan pl;
+  pl.items = 0;
+  pl.bucket = kPlanBuckets - 1;
+  pl.unit_base = -1;
+  pl.blk_os = 1;
+  if (kept > 0 && nos > 0 && !(q.aux[j].flags & kAuxNonfinite)) {
+    const long long chunk = (long long)q.chunk_windows * kWindow;
+    const long long share = (long long)(*q.total_units / (unsigned long long)(8 * q.grid));
+    if (kept > 4 * chunk && kept > share) {
+      const long long chunks = (kept + chunk - 1) / chunk;
+      const int helpers = (int)(chunks < q.max_helpers ? chunks : q.max_helpers);
+      pl.blk_os = helpers;
+      pl.items = (int)(nos * helpers);
+      pl.unit_base = (int)atomicAdd(q.unit_counter, (unsigned)nos);
+      pl.bucket = cost_bucket(kept);
+    } else {
+      const long long pad = ((kept + kWarpTile - 1) / kWarpTile) * kWarpTile;
+      long long b = q.item_cost / pad;
+      b = b < 1 ? 1 : (b > nos ? nos : b);
+      pl.blk_os = (int)b;
+      pl.items = (int)((nos + b - 1) / b);
+      pl.bucket = cost_bucket(pad * b);
+    }
+    atomicAdd(&q.bucket_count[pl.bucket], (unsigned)pl.items);
+  }
+  q.plan[j] = pl;
+}
+
+__global__ void k_plan_scan(PlanParams q) {
+  if (threadIdx.x != 0) return;
+  unsigned run = 0;
+  for (int b = 0; b < kPlanBuckets; ++b) {
+    q.bucket_start[b] = run;
+    q.bucket_cursor[b] = 0;
+    run += q.bucket_count[b];
+  }
+  *q.n_items = (long long)run <= q.item_cap ? (int)run : (int)q.item_cap;
+}
+
+__global__ void __launch_bounds__(128) k_plan_write(PlanParams q) {
+  const int j = blockIdx.x;
+  const JobPlan pl = q.plan[j];
+  if (pl.items == 0) return;
+  __shared__ unsigned s_pos;
+  if (threadIdx.x == 0)
+    s_pos = q.bucket_start[pl.bucket] + atomicAdd(&q.bucket_cursor[pl.bucket], (unsigned)pl.items);
+  __syncthreads();
+  const int nos = q.jobs[j].n_os;
+  for (int k = threadIdx.x; k < pl.items; k += blockDim.x) {
+    const long long pos = (long long)s_pos + k;
+    if (pos >= q.item_cap) break;
+    WorkItem w;
+    w.job = j;
+    if (pl.unit_base >= 0) {
+      const int u = k / pl.blk_os;
+      w.os_begin = u;
+      w.os_count = 1;
+      w.unit = pl.unit_base + u;
+    } else {
+      w.os_begin = k * pl.blk_os;
+      w.os_count = (w.os_begin + pl.blk_os <= nos) ? pl.blk_os : nos - w.os_begin;
+      w.unit = -1;
+    }
+    q.items[pos] = w;
+  }
+}
+
+cudaError_t launch_plan(const PlanParams& q, cudaStream_t s) {
+  if (q.n_jobs <= 0) return cudaSuccess;
+  const int blocks = (q.n_jobs + 255) / 256;
+  k_plan_total<<<blocks, 256, 0, s>>>(q);
+  k_plan_size<<<blocks, 256, 0, s>>>(q);
+  k_plan_scan<<<1, 32, 0, s>>>(q);
+  k_plan_write<<<q.n_jobs, 128, 0, s>>>(q);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------
