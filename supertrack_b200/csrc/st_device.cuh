@@ -9,8 +9,8 @@
 //     consecutive deposits l*kDepPerLane .. l*kDepPerLane+kDepPerLane-1 of the tile:
 //       PX, PY  : x, y as loaded (padding slots hold NaN so the box test rejects them)
 //       PDZ2    : (k_z*d - a_z)^2, +inf when the deposit is outside the box in z
-//       PV      : edep / ((2/3) d)
-//       PKZ     : k_z (uint32)
+//       PVLO/HI : v = edep / ((2/3) d) on the job's fixed-point grid (128-bit integer)
+//       PKEY    : k_z * N*N (the z part of the sphere key); bit 63 flags boundary deposits
 //   * spill tables: one open-addressing table per resident CTA for spheres that do not fit
 //     the CTA's shared-memory table (keys, 128-bit accumulators, used-slot list);
 //   * histograms: int64 counts and float64 y*f(y) sums per bin, one set per histogram.
@@ -58,8 +58,8 @@ struct JobDev {
 
 // Deposits are processed in windows of kWindow consecutive kept deposits (one CTA tile of the
 // fused kernel). A kept deposit is a boundary deposit when a kept deposit of another window lies
-// within distance d of it; the flag travels in the top bit of its PKZ word.
-constexpr uint32_t kBoundaryBit = 0x80000000u;
+// within distance d of it; the flag travels in bit 63 of its PKEY word (keys are below 2^63).
+constexpr unsigned long long kBoundaryBit = 1ull << 63;
 
 // Per-job values produced on the device.
 struct JobAux {
@@ -113,8 +113,9 @@ struct FusedParams {
   const double* PX;
   const double* PY;
   const double* PDZ2;
-  const double* PV;
-  const uint32_t* PKZ;
+  const unsigned long long* PVLO;  // contribution on the job's grid, low 64 bits
+  const unsigned long long* PVHI;  // high 64 bits
+  const unsigned long long* PKEY;  // k_z * N*N, bit 63 = boundary deposit
   // spill tables: gridDim.x tables of gcap slots each
   uint64_t* gkeys;
   unsigned long long* glo;
@@ -152,8 +153,9 @@ struct PrepareParams {
   double* PX;
   double* PY;
   double* PDZ2;
-  double* PV;
-  uint32_t* PKZ;
+  unsigned long long* PVLO;
+  unsigned long long* PVHI;
+  unsigned long long* PKEY;
 };
 
 // Device-side planning of the fused kernel's work items from the kept deposit counts.

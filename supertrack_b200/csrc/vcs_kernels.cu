@@ -26,24 +26,13 @@ __device__ __forceinline__ uint32_t slot_hash(uint64_t key, uint32_t mask) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Lattice index along one axis: k = llrint(a / d) and k as a double, bit-exact with the IEEE
-// quotient. The quotient is first formed as RN(a * RN(1/d)), whose distance to RN(a/d) is below
-// |q| * 2^-51.2; only when q lies within |q| * 2^-50 of a half-integer can the two round to
-// different integers, and then the correctly rounded division decides.
+// Lattice index along one axis, k = llrint(a / d), bit-exact with the IEEE quotient. The fused
+// kernel forms q = RN(a * RN(1/d)), whose distance to RN(a/d) is below |q| * 2^-51.2; it takes
+// k = rint(q) (adding and subtracting 1.5 * 2^52 rounds to the nearest integer, ties to even)
+// unless q lies within 2^-20 of a half-integer, where the correctly rounded division decides.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void lattice_index(double a, double d, double inv_d, uint32_t& k,
-                                              double& kd) {
-  const double kMagic = 0x1.8p52;  // adding it rounds |q| < 2^51 to an integer (ties to even)
-  const double q = st_dmul(a, inv_d);
-  double t = st_dadd(q, kMagic);
-  kd = st_dsub(t, kMagic);
-  const double f = st_dsub(q, kd);  // exact: q minus its nearest integer
-  if (fabs(st_dsub(fabs(f), 0.5)) <= st_dmul(fabs(q), 0x1p-50)) {
-    kd = rint(__ddiv_rn(a, d));
-    t = st_dadd(kd, kMagic);
-  }
-  k = (uint32_t)__double2loint(t);
-}
+constexpr double kMagic = 0x1.8p52;             // adding it rounds |q| < 2^51 to an integer
+constexpr double kRiskBand = 0.5 - 0x1p-20;     // |q - rint(q)| at or above it: decide exactly
 
 // ---------------------------------------------------------------------------------------------
 // Prepare stage (once per track): four launches.
@@ -209,6 +198,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
   constexpr int kWarpsPerBlock = kPrepThreads / 32;
   __shared__ int s_warp[kWarpsPerBlock];
   int64_t run = p.blk_offset[b];  // kept index of the next kept deposit of this block
+  const JobAux A = p.aux[j];
+  const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
   for (int r = 0; r < kPrepSlotsPerBlock / kPrepThreads; ++r) {
     const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
     bool keep = false;
@@ -240,8 +231,11 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       p.PX[dst] = x;
       p.PY[dst] = y;
       p.PDZ2[dst] = st_dmul(dz, dz);
-      p.PV[dst] = __ddiv_rn(J.edep[i], J.denom);
-      p.PKZ[dst] = (uint32_t)(long long)kd;
+      uint64_t lo, hi;
+      to_fixed(__ddiv_rn(J.edep[i], J.denom), E0, &lo, &hi);
+      p.PVLO[dst] = lo;
+      p.PVHI[dst] = hi;
+      p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (J.flagged) {
         p.PZ[dst] = z1;
         cell_insert(p, J, cell_key(x, y, z1, J.cell_size, 0, 0, 0), (uint32_t)(k / kWindow));
@@ -266,8 +260,9 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
   p.PX[dst] = __longlong_as_double(0x7FF8000000000000ll);
   p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
   p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
-  p.PV[dst] = 0.0;
-  p.PKZ[dst] = 0;
+  p.PVLO[dst] = 0;
+  p.PVHI[dst] = 0;
+  p.PKEY[dst] = 0;
 }
 
 // Boundary flags of the kept deposits of flagged jobs: a deposit is a boundary deposit when one of
@@ -291,7 +286,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     bool boundary = false;
     for (int c = 0; c < 27 && !boundary; ++c)
       boundary = cell_foreign(p, J, cell_key(x, y, z, J.cell_size, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win);
-    if (boundary) p.PKZ[dst] |= kBoundaryBit;
+    if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
 }
 
@@ -590,32 +585,51 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
     const int64_t w = wt0 + warp;
     if (w < wt_end) {
       const int64_t tb = J.prep_off + w * kWarpTile + lane;
-      double xv[kDepPerLane], yv[kDepPerLane];
-#pragma unroll
-      for (int p = 0; p < kDepPerLane; ++p) {
-        xv[p] = __ldg(&P.PX[tb + p * 32]);
-        yv[p] = __ldg(&P.PY[tb + p * 32]);
-      }
       uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
       unsigned hitmask = 0, boxmask = 0;
+      // geometry in straight-line blocks of four deposits, so their FP64 chains interleave
 #pragma unroll
-      for (int p = 0; p < kDepPerLane; ++p) {
-        const double x1 = st_dadd(xv[p], sx);
-        const double y1 = st_dadd(yv[p], sy);
-        kxv[p] = 0;
-        kyv[p] = 0;
-        if (fabs(x1) < J.HL && fabs(y1) < J.HL) {
-          boxmask |= 1u << p;
-          const double dz2 = __ldg(&P.PDZ2[tb + p * 32]);
-          const double ax = st_dsub(x1, J.gSO);
-          const double ay = st_dsub(y1, J.gSO);
-          double kdx, kdy;
-          lattice_index(ax, J.d, J.inv_d, kxv[p], kdx);
-          lattice_index(ay, J.d, J.inv_d, kyv[p], kdy);
-          const double ddx = st_dsub(st_dmul(kdx, J.d), ax);
-          const double ddy = st_dsub(st_dmul(kdy, J.d), ay);
+      for (int h4 = 0; h4 < kDepPerLane; h4 += 4) {
+        double ax[4], ay[4], kdx[4], kdy[4];
+        unsigned risk = 0;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const double x1 = st_dadd(__ldg(&P.PX[tb + (h4 + p) * 32]), sx);
+          const double y1 = st_dadd(__ldg(&P.PY[tb + (h4 + p) * 32]), sy);
+          const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
+          boxmask |= (unsigned)inb << (h4 + p);
+          ax[p] = st_dsub(x1, J.gSO);
+          ay[p] = st_dsub(y1, J.gSO);
+          const double qx = st_dmul(ax[p], J.inv_d);
+          const double qy = st_dmul(ay[p], J.inv_d);
+          kdx[p] = st_dsub(st_dadd(qx, kMagic), kMagic);
+          kdy[p] = st_dsub(st_dadd(qy, kMagic), kMagic);
+          const bool near_half = fabs(st_dsub(qx, kdx[p])) >= kRiskBand ||
+                                 fabs(st_dsub(qy, kdy[p])) >= kRiskBand;
+          risk |= (unsigned)(near_half && inb) << p;
+        }
+        if (risk) {
+          // q = RN(a * RN(1/d)) is within |q| 2^-51.2 of RN(a/d), far below 2^-20 for in-box
+          // quotients (|q| < 2^21); only a quotient this close to a half-integer can round
+          // differently, and then the IEEE division decides (rare: lattice-aligned inputs)
+#pragma unroll
+          for (int p = 0; p < 4; ++p) {
+            if (risk & (1u << p)) {
+              kdx[p] = rint(__ddiv_rn(ax[p], J.d));
+              kdy[p] = rint(__ddiv_rn(ay[p], J.d));
+            }
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const double ddx = st_dsub(st_dmul(kdx[p], J.d), ax[p]);
+          const double ddy = st_dsub(st_dmul(kdy[p], J.d), ay[p]);
+          const double dz2 = __ldg(&P.PDZ2[tb + (h4 + p) * 32]);
           const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dz2);
-          if (dist <= J.r2) hitmask |= 1u << p;
+          const bool hit = ((boxmask >> (h4 + p)) & 1u) && dist <= J.r2;
+          hitmask |= (unsigned)hit << (h4 + p);
+          kxv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdx[p], kMagic));
+          kyv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdy[p], kMagic));
         }
       }
       hits += __popc(hitmask);
@@ -627,13 +641,11 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       for (int p = 0; p < kDepPerLane; ++p) {
         if (hitmask & (1u << p)) {
           const int64_t idx = tb + p * 32;
-          const double v = __ldg(&P.PV[idx]);
-          const uint32_t kzw = __ldg(&P.PKZ[idx]);
-          const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N +
-                               (uint64_t)(kzw & ~kBoundaryBit) * J.N2;
+          const uint64_t lo = __ldg(&P.PVLO[idx]);
+          const uint64_t hi = __ldg(&P.PVHI[idx]);
+          const uint64_t kzw = __ldg(&P.PKEY[idx]);
+          const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N + (kzw & ~kBoundaryBit);
           const bool bflag = (kzw & kBoundaryBit) != 0;
-          uint64_t lo, hi;
-          to_fixed(v, F.E0, &lo, &hi);
           if (key == rkey) {
             add128(rlo, rhi, lo, hi);
             rflag |= bflag;
@@ -650,8 +662,9 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
         bool head = lane == 0 || kprev != rkey;
         const bool tail = lane == 31 || knext != rkey;
+        const bool any_run = __any_sync(0xffffffffu, !head && rkey != kEmptyKey);
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; any_run && o < 32; o <<= 1) {
           const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
           const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
           const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
