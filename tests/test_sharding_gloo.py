@@ -1,0 +1,88 @@
+"""Multi-rank sharding logic on CPU: two gloo ranks each take their LPT share of the jobs, compute
+their spectra (with the CPU oracle standing in for the GPU of each rank), and all-reduce them;
+the result equals the single-process spectrum of all jobs."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from supertrack_b200.sharding import lpt_assign, shard
+
+
+def test_lpt_balances_and_covers():
+    rs = np.random.default_rng(0)
+    costs = np.exp(rs.normal(10, 1.5, 500))
+    for world in (1, 2, 3, 8):
+        owner = lpt_assign(costs, world)
+        assert set(owner.tolist()) <= set(range(world))
+        loads = np.array([costs[owner == r].sum() for r in range(world)])
+        assert loads.max() <= costs.sum() / world + costs.max() + 1e-6
+        got = sorted(sum((shard(costs, r, world) for r in range(world)), []))
+        assert got == list(range(len(costs)))
+    assert np.array_equal(lpt_assign(costs, 4), lpt_assign(costs, 4))  # deterministic
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out_path):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "oracle"))
+    import torch.distributed as dist
+    import pyoracle as po
+    import supertrack_b200.workloads as W
+    from supertrack_b200.sharding import reduce_spectra, shard
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w = W.config0(n_tracks=12, n_os=3)
+        costs = w.sizes * w.n_os
+        e = po.edges(*w.hists[0])
+        counts = np.zeros(len(e) - 1, dtype=np.int64)
+        yfy = np.zeros(len(e) - 1)
+        for j in shard(costs, rank, world):
+            x, y, z, ed = [a.numpy() for a in w.job_arrays(j)]
+            sx = po.shifts(2500.0, 10.0, True, int(w.seed[j]), j, int(w.n_os[j]))
+            po.run_job(x, y, z, ed, half_length=2500.0, sphere_diameter=10.0, sxsy=sx,
+                       edges_arr=e, zshift=w.zshift, counts=counts, yfy=yfy)
+        c, y = reduce_spectra(counts, yfy)
+        if rank == 0:
+            np.savez(out_path, counts=c, yfy=y)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_spectrum_equals_single_process(tmp_path):
+    import pyoracle as po
+    import supertrack_b200.workloads as W
+    out = str(tmp_path / "r.npz")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    got = np.load(out)
+    w = W.config0(n_tracks=12, n_os=3)
+    e = po.edges(*w.hists[0])
+    counts = np.zeros(len(e) - 1, dtype=np.int64)
+    yfy = np.zeros(len(e) - 1)
+    for j in range(w.n_jobs):
+        x, y, z, ed = [a.numpy() for a in w.job_arrays(j)]
+        sx = po.shifts(2500.0, 10.0, True, int(w.seed[j]), j, int(w.n_os[j]))
+        po.run_job(x, y, z, ed, half_length=2500.0, sphere_diameter=10.0, sxsy=sx, edges_arr=e,
+                   zshift=w.zshift, counts=counts, yfy=yfy)
+    assert np.array_equal(got["counts"], counts)
+    np.testing.assert_allclose(got["yfy"], yfy, rtol=1e-12)
