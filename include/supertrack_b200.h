@@ -194,6 +194,27 @@ ST_API st_status st_jobs_count(const st_ctx* ctx, int32_t* n);
  * the reference's per-oversample reduced VolumeEdepPair (Histogram.cu:150-153). */
 ST_API st_status st_run_export(st_ctx* ctx, st_sphere* spheres_out, int64_t cap, int64_t* n_out);
 
+/* --- superimposition without device allocation ------------------------------------------------
+ * No counterpart in the reference. For callers that must not allocate device memory on their
+ * path: cudaFree synchronises the whole device and stalls every other stream (a serving thread
+ * sharing the GPU cannot afford that), embedding frameworks often own all device memory through
+ * their own pool, and work recorded into CUDA graphs may not allocate between launches. The call
+ * allocates nothing: it works in a fixed scratch array compiled into the library
+ * (st_noalloc_scratch_bytes() bytes, about 6.2 MB, held by every GPU that loads the library
+ * until the process exits). Limits: one device-resident track (track->on_device != 0) of at
+ * most 16384 deposits, at most 65536 oversamples, a histogram of at most 4096 bins; larger
+ * requests return ST_ERR_CAPACITY. d_counts (int64) and d_yfy (float64) are device arrays of
+ * nbins that the call adds into. desc->hist_id is ignored. Work is enqueued on `stream` (NULL:
+ * the legacy default stream) on the current device, which is synchronised before returning.
+ * The first call on each device resolves the scratch array's device address and should come
+ * before any stream capture. All calls share the one scratch array, so calls that overlap on the
+ * GPU race: issue them on one stream or serialise them. */
+ST_API st_status st_superimpose_noalloc(const st_track_view* track, const st_job_desc* desc,
+                                        int32_t hist_type, int32_t nbins, float lower,
+                                        float upper, int64_t* d_counts, double* d_yfy,
+                                        void* stream, st_job_stats* stats_out);
+ST_API int64_t st_noalloc_scratch_bytes(void);
+
 /* --- macro-level run (SuperTrackManager) ----------------------------------------------------- */
 
 typedef struct {

@@ -119,6 +119,11 @@ SIGNATURES = [
     ("st_measure_fp64_peak", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("st_jobs_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("st_run_export", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
+    ("st_superimpose_noalloc", C.c_int, [C.POINTER(st_track_view), C.POINTER(st_job_desc),
+                                         C.c_int32, C.c_int32, C.c_float, C.c_float,
+                                         C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(st_job_stats)]),
+    ("st_noalloc_scratch_bytes", C.c_int64, []),
     ("st_run_macro", C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                C.c_int32, C.POINTER(st_run_info), C.c_char_p, C.c_size_t]),
     ("st_track_file_write", C.c_int, [C.c_char_p, C.c_uint64, C.c_void_p, C.c_uint64,
