@@ -129,7 +129,7 @@ def gen_proton(g, sizes: torch.Tensor, device) -> Tuple[torch.Tensor, ...]:
     key = tid * (1 << 20) + wid
     first_of_walk = torch.ones(total, dtype=torch.bool, device=device)
     first_of_walk[1:] = key[1:] != key[:-1]
-    cs = torch.cumsum(dsteps, 0)
+    cs = torch.stack([torch.cumsum(dsteps[:, k].contiguous(), 0) for k in range(3)], 1)
     walk_begin_idx = torch.cummax(torch.where(first_of_walk, torch.arange(total, device=device),
                                               torch.zeros_like(local)), 0).values
     within = cs - cs[walk_begin_idx] + dsteps[walk_begin_idx]
