@@ -164,6 +164,9 @@ ST_API st_status st_hist_reset(st_ctx* ctx, int32_t hist_id);
 ST_API st_status st_hist_read_all(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap,
                                   int64_t* n_bins);
 ST_API st_status st_hist_offset(const st_ctx* ctx, int32_t hist_id, int64_t* first_bin);
+/* As st_hist_read_all, but only enqueued on the context's stream (host arrays should be pinned);
+ * a run in flight (st_run_async) reports completion only after these copies. */
+ST_API st_status st_hist_read_all_async(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap);
 ST_API st_status st_hist_nbins(const st_ctx* ctx, int32_t hist_id, int32_t* nbins);
 ST_API st_status st_hist_edges_of(const st_ctx* ctx, int32_t hist_id, double* edges);
 
@@ -179,6 +182,14 @@ ST_API st_status st_job_submit(st_ctx* ctx, const st_track_view* track, const st
  * with its own launches and a host synchronisation (the reference's per-task loop shape). */
 ST_API st_status st_run(st_ctx* ctx, int32_t mode);
 ST_API st_status st_job_stats_get(st_ctx* ctx, int32_t job_id, st_job_stats* out);
+/* Asynchronous form of st_run(ST_RUN_BATCHED): enqueues the run on the context's stream and
+ * returns; st_run_query reports whether it finished (and then collects its statistics and
+ * status), st_run_finish waits for it. One run per context may be in flight. */
+ST_API st_status st_run_async(st_ctx* ctx);
+ST_API st_status st_run_query(st_ctx* ctx, int32_t* done);
+ST_API st_status st_run_finish(st_ctx* ctx);
+/* Forgets every histogram of the context (device memory is kept for reuse); ids restart at 0. */
+ST_API st_status st_hists_clear(st_ctx* ctx);
 /* Queues n jobs at once (tracks[i] with descs[i]); job_ids may be NULL. */
 ST_API st_status st_job_submit_many(st_ctx* ctx, int32_t n, const st_track_view* tracks,
                                     const st_job_desc* descs, int32_t* job_ids);
@@ -193,6 +204,47 @@ ST_API st_status st_jobs_count(const st_ctx* ctx, int32_t* n);
  * energy, in no particular order; spheres_out has room for cap records. The exported list is
  * the reference's per-oversample reduced VolumeEdepPair (Histogram.cu:150-153). */
 ST_API st_status st_run_export(st_ctx* ctx, st_sphere* spheres_out, int64_t cap, int64_t* n_out);
+
+/* --- serving: continuous batching of arriving jobs ------------------------------------------
+ * Replaces the reference's static, fork-per-thread task loop (SuperTrackManager.cu:49-102) for
+ * jobs that arrive over time. A worker thread admits queued jobs while their device footprint
+ * (prepared records, boundary cells, histogram) fits the budget, batches them into one launch
+ * sequence on one of two contexts (two streams: the next batch is enqueued while the previous one
+ * is still on the GPU), and on completion copies each job's spectrum to the caller's host arrays
+ * and records its latency. Tracks must be device-resident and stay valid until completion. */
+typedef struct st_server st_server;
+typedef struct {
+  uint64_t tag;              /* the caller's tag from st_server_submit                      */
+  int32_t status;            /* st_status of the job                                        */
+  int32_t batch;             /* index of the batch that ran it                              */
+  int64_t submit_ns;         /* steady-clock times: submitted, its batch launched, done     */
+  int64_t start_ns;
+  int64_t done_ns;
+} st_completion;
+
+ST_API st_status st_server_create(int32_t device, int64_t budget_bytes, int64_t max_track_deposits,
+                                  int32_t max_batch_jobs, st_server** out);
+ST_API st_status st_server_destroy(st_server* server);
+/* Device bytes a job is charged against the budget while its batch is in flight. */
+ST_API st_status st_server_job_footprint(const st_track_view* track, const st_job_desc* desc,
+                                         int32_t nbins, int64_t* bytes);
+/* Bytes of the budget set aside for the two contexts' spill tables (per-sphere scratch). */
+ST_API st_status st_server_reserve_bytes(const st_server* server, int64_t* bytes);
+/* Queues one job. counts_out (int64[nbins]) and yfy_out (float64[nbins]) receive its spectrum. */
+ST_API st_status st_server_submit(st_server* server, const st_track_view* track,
+                                  const st_job_desc* desc, int32_t hist_type, int32_t nbins,
+                                  float lower, float upper, int64_t* counts_out, double* yfy_out,
+                                  uint64_t tag);
+/* Submits n jobs from a server-side thread at start + arrival_ns[i] (steady clock), returning at
+ * once; outputs are counts_out/yfy_out + i*nbins. All jobs share one histogram specification. */
+ST_API st_status st_server_replay(st_server* server, int32_t n, const st_track_view* tracks,
+                                  const st_job_desc* descs, const int64_t* arrival_ns,
+                                  int32_t hist_type, int32_t nbins, float lower, float upper,
+                                  int64_t* counts_out, double* yfy_out);
+/* Moves up to cap finished-job records into out; n_out receives the number moved. */
+ST_API st_status st_server_poll(st_server* server, st_completion* out, int32_t cap, int32_t* n_out);
+/* Waits until every submitted (and replayed) job has completed, or timeout_ms elapses. */
+ST_API st_status st_server_drain(st_server* server, int64_t timeout_ms);
 
 /* --- superimposition without device allocation ------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their

@@ -23,7 +23,7 @@ __all__ = [
     "StError", "Context", "geometry", "hist_edges", "philox4x32_10", "oversample_shifts",
     "INIReader", "SphericalGeometry", "Histogram", "VoxelConstrainedSphereMethod",
     "SuperTrackManager", "run_macro", "macro_tasks", "write_track_file", "ZSHIFT",
-    "HIST_TYPES",
+    "HIST_TYPES", "Server",
 ]
 
 ZSHIFT = {"plus": ST_ZSHIFT_PLUS, "minus": ST_ZSHIFT_MINUS, "none": ST_ZSHIFT_NONE}
@@ -321,6 +321,23 @@ class Context:
         m = {"batched": ST_RUN_BATCHED, "plain": ST_RUN_PLAIN}[mode]
         self._check(lib().st_run(self._h, m), "st_run")
 
+    def run_async(self) -> None:
+        """Enqueues a batched run of the queued jobs and returns at once."""
+        self._check(lib().st_run_async(self._h), "st_run_async")
+
+    def query(self) -> bool:
+        """True once the run enqueued by :meth:`run_async` has finished (statistics collected)."""
+        done = C.c_int32(0)
+        self._check(lib().st_run_query(self._h, C.byref(done)), "st_run_query")
+        return bool(done.value)
+
+    def finish(self) -> None:
+        """Waits for the run enqueued by :meth:`run_async`."""
+        self._check(lib().st_run_finish(self._h), "st_run_finish")
+
+    def clear_histograms(self) -> None:
+        self._check(lib().st_hists_clear(self._h), "st_hists_clear")
+
     def run_export(self, cap: int = 1 << 20) -> np.ndarray:
         out = np.zeros(cap, dtype=SPHERE_DTYPE)
         n = C.c_int64(0)
@@ -340,6 +357,122 @@ class Context:
         n = C.c_int32()
         self._check(lib().st_jobs_count(self._h, C.byref(n)), "st_jobs_count")
         return n.value
+
+
+COMPLETION_DTYPE = np.dtype([("tag", "<u8"), ("status", "<i4"), ("batch", "<i4"),
+                             ("submit_ns", "<i8"), ("start_ns", "<i8"), ("done_ns", "<i8")])
+
+
+class Server:
+    """Continuous-batching server (st_server_*): jobs on device-resident tracks are queued,
+    admitted by device footprint against ``budget_bytes`` and run in batches on two alternating
+    contexts; each job's spectrum lands in its own host arrays."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 150_000_000_000,
+                 max_track_deposits: int = 2_000_000, max_batch_jobs: int = 4096):
+        h = C.c_void_p()
+        check(lib().st_server_create(device, int(budget_bytes), int(max_track_deposits),
+                                     int(max_batch_jobs), C.byref(h)), "st_server_create")
+        self._h = h
+        self._keep: List[object] = []
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().st_server_destroy(self._h), "st_server_destroy")
+            self._h = None
+            self._keep = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _view(x, y, z, edep) -> _capi.st_track_view:
+        v = _capi.st_track_view()
+        v.x, v.y, v.z, v.edep = [a if isinstance(a, int) else a.data_ptr() for a in (x, y, z, edep)]
+        v.n = int(x.numel())
+        v.on_device = 1
+        return v
+
+    @staticmethod
+    def _desc(half_length, sphere_diameter, n_oversamples, seed, track_id, shift_track, zshift):
+        d = _capi.st_job_desc()
+        d.half_length = half_length
+        d.sphere_diameter = sphere_diameter
+        d.zshift = ZSHIFT[zshift] if isinstance(zshift, str) else int(zshift)
+        d.shift_track = int(bool(shift_track))
+        d.n_oversamples = n_oversamples
+        d.hist_id = -1
+        d.seed = seed & 0xFFFFFFFFFFFFFFFF
+        d.track_id = track_id & 0xFFFFFFFFFFFFFFFF
+        return d
+
+    def submit(self, x, y, z, edep, *, half_length: float, sphere_diameter: float,
+               n_oversamples: int, hist: Tuple[str, int, float, float], counts: np.ndarray,
+               yfy: np.ndarray, seed: int = 0, track_id: int = 0, shift_track: bool = True,
+               zshift: str = "plus", tag: int = 0) -> None:
+        """Queues one job on CUDA tensors x, y, z, edep (float64); ``counts`` (int64) and ``yfy``
+        (float64) receive its spectrum and must stay alive until it completes."""
+        kind, nb, lo, hi = hist
+        if counts.dtype != np.int64 or yfy.dtype != np.float64 or len(counts) < nb or len(yfy) < nb:
+            raise ValueError("counts must be int64[nbins] and yfy float64[nbins]")
+        v = self._view(x, y, z, edep)
+        d = self._desc(half_length, sphere_diameter, n_oversamples, seed, track_id, shift_track,
+                       zshift)
+        self._keep.extend([x, y, z, edep, counts, yfy])
+        check(lib().st_server_submit(self._h, C.byref(v), C.byref(d), HIST_TYPES[kind], nb, lo, hi,
+                                     _ptr(counts), _ptr(yfy), tag), "st_server_submit")
+
+    def replay(self, views: np.ndarray, descs: np.ndarray, arrival_ns: np.ndarray,
+               hist: Tuple[str, int, float, float], counts: np.ndarray, yfy: np.ndarray) -> None:
+        """Releases job i at ``arrival_ns[i]`` after the call (server-side thread); ``views`` and
+        ``descs`` are ctypes arrays of st_track_view / st_job_desc, ``counts``/``yfy`` are
+        (n, nbins) arrays. Completion tags are the job indices."""
+        kind, nb, lo, hi = hist
+        n = len(arrival_ns)
+        arr = np.ascontiguousarray(arrival_ns, dtype=np.int64)
+        if counts.shape != (n, nb) or yfy.shape != (n, nb):
+            raise ValueError("counts and yfy must be (n_jobs, nbins)")
+        self._keep.extend([views, descs, arr, counts, yfy])
+        check(lib().st_server_replay(self._h, n, C.cast(views, C.c_void_p),
+                                     C.cast(descs, C.c_void_p), _ptr(arr), HIST_TYPES[kind], nb,
+                                     lo, hi, _ptr(counts), _ptr(yfy)), "st_server_replay")
+
+    def reserve_bytes(self) -> int:
+        """Budget bytes set aside for the spill tables of the server's two contexts."""
+        b = C.c_int64(0)
+        check(lib().st_server_reserve_bytes(self._h, C.byref(b)), "st_server_reserve_bytes")
+        return b.value
+
+    @staticmethod
+    def job_footprint(view: _capi.st_track_view, desc: _capi.st_job_desc, nbins: int) -> int:
+        """Device bytes a job is charged against the budget while in flight."""
+        b = C.c_int64(0)
+        check(lib().st_server_job_footprint(C.byref(view), C.byref(desc), nbins, C.byref(b)),
+              "st_server_job_footprint")
+        return b.value
+
+    def drain(self, timeout_s: float = 600.0) -> None:
+        check(lib().st_server_drain(self._h, int(timeout_s * 1000)), "st_server_drain")
+
+    def poll(self, cap: int = 1 << 16) -> np.ndarray:
+        """Completion records of finished jobs (each returned once)."""
+        out = np.zeros(cap, dtype=COMPLETION_DTYPE)
+        got = []
+        while True:
+            n = C.c_int32(0)
+            check(lib().st_server_poll(self._h, _ptr(out), cap, C.byref(n)), "st_server_poll")
+            got.append(out[: n.value].copy())
+            if n.value < cap:
+                return np.concatenate(got)
 
 
 # ------------------------------------------------------------------------------------------------

@@ -67,6 +67,11 @@ class st_sphere(C.Structure):
     _fields_ = [("key", C.c_uint64), ("y", C.c_double), ("os", C.c_int32), ("job", C.c_int32)]
 
 
+class st_completion(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("status", C.c_int32), ("batch", C.c_int32),
+                ("submit_ns", C.c_int64), ("start_ns", C.c_int64), ("done_ns", C.c_int64)]
+
+
 class st_run_info(C.Structure):
     _fields_ = [("n_tracks", C.c_int64), ("n_oversamples", C.c_int64),
                 ("n_effective", C.c_int64), ("random_seed", C.c_int64),
@@ -119,6 +124,25 @@ SIGNATURES = [
     ("st_measure_fp64_peak", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("st_jobs_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("st_run_export", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
+    ("st_run_async", C.c_int, [C.c_void_p]),
+    ("st_run_query", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("st_run_finish", C.c_int, [C.c_void_p]),
+    ("st_hists_clear", C.c_int, [C.c_void_p]),
+    ("st_hist_read_all_async", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    ("st_server_create", C.c_int, [C.c_int32, C.c_int64, C.c_int64, C.c_int32,
+                                   C.POINTER(C.c_void_p)]),
+    ("st_server_destroy", C.c_int, [C.c_void_p]),
+    ("st_server_job_footprint", C.c_int, [C.POINTER(st_track_view), C.POINTER(st_job_desc),
+                                          C.c_int32, C.POINTER(C.c_int64)]),
+    ("st_server_reserve_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    ("st_server_submit", C.c_int, [C.c_void_p, C.POINTER(st_track_view), C.POINTER(st_job_desc),
+                                   C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_void_p,
+                                   C.c_void_p, C.c_uint64]),
+    ("st_server_replay", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_void_p,
+                                   C.c_void_p]),
+    ("st_server_poll", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    ("st_server_drain", C.c_int, [C.c_void_p, C.c_int64]),
     ("st_superimpose_noalloc", C.c_int, [C.POINTER(st_track_view), C.POINTER(st_job_desc),
                                          C.c_int32, C.c_int32, C.c_float, C.c_float,
                                          C.c_void_p, C.c_void_p, C.c_void_p,

@@ -34,9 +34,13 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// Grow-only device buffer. A buffer that has to grow again takes at least half as much more, so
+// that contexts running batches of changing size (serving) reallocate rarely: cudaFree waits
+// for the whole device.
 cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return cudaSuccess;
+  if (b.bytes > 0) bytes = std::max(bytes, b.bytes + b.bytes / 2);
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
@@ -132,6 +136,14 @@ struct st_ctx {
   st::PlanParams cache_plan{};
   int chunk_windows = 4;      // windows (4096 deposits each) per chunk of a shared unit
   int max_helpers = 32;       // helper items per shared unit
+
+  // results of an enqueued run are copied into pinned buffers and picked up at finish
+  JobAux* h_aux = nullptr;
+  size_t h_aux_cap = 0;
+  int* h_err = nullptr;           // 4 ints + export count (8 bytes)
+  bool pending = false;
+  size_t pend_first = 0, pend_last = 0;
+  bool pend_export = false;
 };
 
 namespace {
@@ -437,17 +449,14 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   return ST_OK;
 }
 
-// Runs jobs [first, last) of the context in one prepare launch and one fused launch.
-st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int64_t ex_cap,
-                    int64_t* ex_n) {
-  if (first >= last) {
-    if (ex_n) *ex_n = 0;
-    return ST_OK;
-  }
+// Enqueues jobs [first, last) of the context: uploads, prepare and plan launches, the fused
+// launch, and the copy of the job counters and error flags into pinned host buffers. Nothing
+// waits; finish_range picks the results up.
+st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, int64_t ex_cap) {
   const size_t nj = last - first;
-  const bool reuse = !ex_out && c->cache_valid && c->cache_first == first && c->cache_last == last;
+  const bool reuse = !want_export && c->cache_valid && c->cache_first == first && c->cache_last == last;
   if (!reuse) {
-    st_status s = build_tables(c, first, last, ex_out != nullptr);
+    st_status s = build_tables(c, first, last, want_export);
     if (s != ST_OK) { c->cache_valid = false; return s; }
   }
   {
@@ -472,7 +481,7 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
 
   st::FusedParams fp = c->cache_fp;
-  if (ex_out) {
+  if (want_export) {
     ST_CUDA(ensure(c->ex_buf, (size_t)std::max<int64_t>(ex_cap, 1) * sizeof(st::SphereRecord)), "export buffer");
     ST_CUDA(ensure(c->ex_count, 16), "export counter");
     ST_CUDA(cudaMemsetAsync(c->ex_count.p, 0, 16, c->stream), "export counter");
@@ -489,14 +498,36 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
   if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
   c->launches += (c->cache_blocks > 0 ? 1 : 0) + (c->cache_grid > 0 ? 1 : 0);
 
-  // ---- results
-  std::vector<JobAux> aux(nj);
-  ST_CUDA(cudaMemcpyAsync(aux.data(), c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
-  int errflags[4] = {0, 0, 0, 0};
-  ST_CUDA(cudaMemcpyAsync(errflags, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
+  // ---- results into pinned host buffers
+  if (c->h_aux_cap < nj) {
+    if (c->h_aux) cudaFreeHost(c->h_aux);
+    c->h_aux = nullptr;
+    c->h_aux_cap = 0;
+    ST_CUDA(cudaMallocHost(&c->h_aux, std::max<size_t>(nj, 1024) * sizeof(JobAux)), "pinned aux");
+    c->h_aux_cap = std::max<size_t>(nj, 1024);
+  }
+  if (!c->h_err) ST_CUDA(cudaMallocHost(&c->h_err, 32), "pinned flags");
+  ST_CUDA(cudaMemcpyAsync(c->h_aux, c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
+  ST_CUDA(cudaMemcpyAsync(c->h_err, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
+  if (want_export) ST_CUDA(cudaMemcpyAsync(c->h_err + 4, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
+  ST_CUDA(cudaEventRecord(c->ev[3], c->stream), "event");
+  c->pending = true;
+  c->pend_first = first;
+  c->pend_last = last;
+  c->pend_export = want_export;
+  return ST_OK;
+}
+
+// Waits for the enqueued run and turns its counters and flags into job statistics and a status.
+st_status finish_range(st_ctx* c, st_sphere* ex_out, int64_t ex_cap, int64_t* ex_n) {
+  if (!c->pending) return ST_OK;
+  c->pending = false;
+  const size_t first = c->pend_first, last = c->pend_last, nj = last - first;
+  ST_CUDA(cudaEventSynchronize(c->ev[3]), "run");
+  const JobAux* aux = c->h_aux;
+  int errflags[4] = {c->h_err[0], c->h_err[1], c->h_err[2], c->h_err[3]};
   unsigned long long exn = 0;
-  if (ex_out) ST_CUDA(cudaMemcpyAsync(&exn, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
-  ST_CUDA(cudaStreamSynchronize(c->stream), "run");
+  if (c->pend_export) std::memcpy(&exn, c->h_err + 4, 8);
   if (c->timing) {
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
@@ -545,6 +576,22 @@ st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int
     if (ex_n) *ex_n = (int64_t)exn;
   }
   return result;
+}
+
+// Runs jobs [first, last) of the context in one batched launch sequence and waits for it.
+st_status run_range(st_ctx* c, size_t first, size_t last, st_sphere* ex_out, int64_t ex_cap,
+                    int64_t* ex_n) {
+  if (first >= last) {
+    if (ex_n) *ex_n = 0;
+    return ST_OK;
+  }
+  if (c->pending) {
+    st_status s = finish_range(c, nullptr, 0, nullptr);
+    if (s != ST_OK) return s;
+  }
+  st_status s = launch_range(c, first, last, ex_out != nullptr, ex_cap);
+  if (s != ST_OK) return s;
+  return finish_range(c, ex_out, ex_cap, ex_n);
 }
 
 }  // namespace
@@ -672,6 +719,8 @@ st_status st_ctx_destroy(st_ctx* c) {
                     &c->h_yfy, &c->h_edges};
   for (DevBuf* b : bufs) release(*b);
   for (auto& e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->h_aux) cudaFreeHost(c->h_aux);
+  if (c->h_err) cudaFreeHost(c->h_err);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return ST_OK;
@@ -750,7 +799,6 @@ st_status st_hist_create(st_ctx* c, int32_t type, int32_t nbins, float lower, fl
   ST_CUDA(cudaMemcpyAsync((double*)c->h_edges.p + h.eoff, h.edges.data(), h.edges.size() * 8, cudaMemcpyHostToDevice, c->stream), "histogram edges");
   ST_CUDA(cudaMemsetAsync((unsigned long long*)c->h_counts.p + h.off, 0, (size_t)nbins * 8, c->stream), "histogram counts");
   ST_CUDA(cudaMemsetAsync((double*)c->h_yfy.p + h.off, 0, (size_t)nbins * 8, c->stream), "histogram yfy");
-  ST_CUDA(cudaStreamSynchronize(c->stream), "histogram create");
   c->h_bins += nbins;
   c->h_edge_total += nbins + 1;
   c->hists.push_back(std::move(h));
@@ -783,6 +831,18 @@ st_status st_hist_read_all(st_ctx* c, int64_t* counts, double* yfy, int64_t cap,
 st_status st_hist_offset(const st_ctx* c, int32_t hist_id, int64_t* first_bin) {
   if (!c || !first_bin || hist_id < 0 || hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
   *first_bin = c->hists[hist_id].off;
+  return ST_OK;
+}
+
+st_status st_hist_read_all_async(st_ctx* c, int64_t* counts, double* yfy, int64_t cap) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  if (cap < c->h_bins) return ST_ERR_CAPACITY;
+  if (c->h_bins == 0) return ST_OK;
+  cudaSetDevice(c->device);
+  if (counts) ST_CUDA(cudaMemcpyAsync(counts, c->h_counts.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, c->h_yfy.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  // an enqueued run now completes only once the copies have landed
+  if (c->pending) ST_CUDA(cudaEventRecord(c->ev[3], c->stream), "event");
   return ST_OK;
 }
 
@@ -857,6 +917,42 @@ st_status st_run_export(st_ctx* c, st_sphere* spheres_out, int64_t cap, int64_t*
   c->t_prep = c->t_fused = 0;
   c->launches = 0;
   return run_range(c, first_unrun(c), c->jobs.size(), spheres_out, cap, n_out);
+}
+
+st_status st_run_async(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  if (c->pending) return ST_ERR_STATE;
+  c->t_prep = c->t_fused = 0;
+  c->launches = 0;
+  const size_t first = first_unrun(c), last = c->jobs.size();
+  if (first >= last) return ST_OK;
+  return launch_range(c, first, last, false, 0);
+}
+
+st_status st_run_query(st_ctx* c, int32_t* done) {
+  if (!c || !done) return ST_ERR_INVALID_ARGUMENT;
+  if (!c->pending) { *done = 1; return ST_OK; }
+  const cudaError_t e = cudaEventQuery(c->ev[3]);
+  if (e == cudaErrorNotReady) { *done = 0; return ST_OK; }
+  *done = 1;
+  return finish_range(c, nullptr, 0, nullptr);
+}
+
+st_status st_run_finish(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  return finish_range(c, nullptr, 0, nullptr);
+}
+
+st_status st_hists_clear(st_ctx* c) {
+  if (!c) return ST_ERR_INVALID_ARGUMENT;
+  if (c->pending) return ST_ERR_STATE;
+  c->hists.clear();
+  c->h_bins = 0;
+  c->h_edge_total = 0;
+  c->cache_valid = false;
+  return ST_OK;
 }
 
 st_status st_job_stats_get(st_ctx* c, int32_t job_id, st_job_stats* out) {

@@ -319,3 +319,27 @@ def test_no_device_is_reported_not_crashed():
     with pytest.raises(st.StError) as e:
         st.Context(0)
     assert e.value.status == _capi.ST_ERR_NO_DEVICE
+
+
+def test_server_job_footprint():
+    """The admission charge of a served job: grows with deposits, oversamples and bins; the
+    boundary-cell hash of window-flagged jobs (fine lattice, >8192 deposits, >=4 oversamples)
+    is charged on top; bad geometry is refused."""
+    def foot(n, d=10.0, os_=10, nbins=200, hl=2500.0):
+        v = _capi.st_track_view()
+        v.n = n
+        v.on_device = 1
+        q = _capi.st_job_desc()
+        q.half_length = hl
+        q.sphere_diameter = d
+        q.n_oversamples = os_
+        b = _capi.C.c_int64(0)
+        rc = _capi.lib().st_server_job_footprint(_capi.C.byref(v), _capi.C.byref(q), nbins,
+                                                 _capi.C.byref(b))
+        return rc, b.value
+    rc, b0 = foot(1000)
+    assert rc == 0 and b0 >= 80 * 1000
+    assert foot(2000)[1] > b0 and foot(1000, os_=100)[1] > b0 and foot(1000, nbins=3000)[1] > b0
+    # 1e5 deposits: flagged for d = 10 nm (N = 500), not for d = 1000 nm (N = 5)
+    assert foot(100_000, d=10.0)[1] - foot(100_000, d=1000.0)[1] >= 16 * 2 * 100_000
+    assert foot(1000, d=-1.0)[0] == _capi.ST_ERR_BAD_GEOMETRY
