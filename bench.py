@@ -285,6 +285,7 @@ def ours(args, rank, world):
     torch.cuda.set_stream(stream)
     w, desc = make_workload(args.config, dev, 1000 * rank, args.scale)
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()   # the generator's temporaries: the context sizes from free memory
     ctx = st.Context(dev.index, stream=stream.cuda_stream)
     hist_ids = [ctx.histogram(*h) for h in w.hists]
     submit_all(ctx, w, hist_ids, True, (w.x, w.y, w.z, w.edep))

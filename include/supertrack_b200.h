@@ -137,15 +137,32 @@ ST_API st_status st_ctx_destroy(st_ctx* ctx);
 ST_API st_status st_ctx_set_stream(st_ctx* ctx, void* stream);
 ST_API st_status st_ctx_last_error(const st_ctx* ctx, char* buf, size_t len);
 ST_API int32_t st_ctx_sm_count(const st_ctx* ctx);
-/* Enables CUDA-event timing of the prepare and fused kernels inside st_run. */
+/* Kept for callers that switch timing on: every run is timed with CUDA events. */
 ST_API st_status st_ctx_enable_timing(st_ctx* ctx, int32_t on);
-/* Milliseconds of the last st_run: prepare kernel, fused kernel, and number of kernel launches. */
+/* Milliseconds of the last st_run / st_run_async (summed over its launches): prepare and plan
+ * kernels, fused kernel (from its start, after any st_ctx_order_after wait), and the number of
+ * kernel launches. */
 ST_API st_status st_ctx_last_timing(const st_ctx* ctx, float* prepare_ms, float* fused_ms,
                                     int32_t* launches);
 /* Measured FP64 add/multiply issue rate of the device (operations per second). */
 ST_API st_status st_measure_fp64_peak(st_ctx* ctx, double* ops_per_second);
 /* Tuning knobs: target deposit*oversamples per work item, resident CTAs (0 = one per SM). */
 ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid);
+/* Named work-planning parameters (all take effect at the next run):
+ *   item_cost          deposit*oversamples per private work item            (default 262144)
+ *   grid               resident CTAs of the fused kernel, 0 = one per SM     (default 0)
+ *   chunk_windows      windows of 4096 kept deposits per chunk of a shared unit   (default 4)
+ *   max_helpers        helper items per shared unit                          (default 32)
+ *   share_divisor      a job runs as shared units (one per oversample) when its kept deposits
+ *                      exceed batch units / (share_divisor * grid); 0 = never (default 8)
+ *   shared_min_chunks  ... and exceed this many chunks                       (default 4)
+ *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to
+ *                      hold every sphere of the batch's largest job); the grid shrinks to fit;
+ *                      0 = 30% of free device memory, at most 48 GB          (default 0)
+ * st_ctx_get_param also reads "last_grid" (CTAs of the last fused launch) and "spill_slots"
+ * (slots of each CTA's spill table). */
+ST_API st_status st_ctx_set_param(st_ctx* ctx, const char* name, int64_t value);
+ST_API st_status st_ctx_get_param(const st_ctx* ctx, const char* name, int64_t* value);
 
 /* --- histograms (device accumulators) ------------------------------------------------------ */
 
@@ -164,9 +181,11 @@ ST_API st_status st_hist_reset(st_ctx* ctx, int32_t hist_id);
 ST_API st_status st_hist_read_all(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap,
                                   int64_t* n_bins);
 ST_API st_status st_hist_offset(const st_ctx* ctx, int32_t hist_id, int64_t* first_bin);
-/* As st_hist_read_all, but only enqueued on the context's stream (host arrays should be pinned);
- * a run in flight (st_run_async) reports completion only after these copies. */
-ST_API st_status st_hist_read_all_async(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap);
+/* Copies bins [first_bin, first_bin + n_bins) of the context's histograms (in creation order,
+ * see st_hist_offset) to counts/yfy, enqueued on the context's stream only (host arrays should
+ * be pinned); a run in flight (st_run_async) reports completion only after these copies. */
+ST_API st_status st_hist_read_bins_async(st_ctx* ctx, int64_t first_bin, int64_t n_bins,
+                                         int64_t* counts, double* yfy);
 ST_API st_status st_hist_nbins(const st_ctx* ctx, int32_t hist_id, int32_t* nbins);
 ST_API st_status st_hist_edges_of(const st_ctx* ctx, int32_t hist_id, double* edges);
 
@@ -188,6 +207,9 @@ ST_API st_status st_job_stats_get(st_ctx* ctx, int32_t job_id, st_job_stats* out
 ST_API st_status st_run_async(st_ctx* ctx);
 ST_API st_status st_run_query(st_ctx* ctx, int32_t* done);
 ST_API st_status st_run_finish(st_ctx* ctx);
+/* The fused kernel of ctx's next run starts only after the fused kernel last enqueued by other
+ * (a context on another stream of the same device) has finished; its prepare stage may overlap. */
+ST_API st_status st_ctx_order_after(st_ctx* ctx, const st_ctx* other);
 /* Forgets every histogram of the context (device memory is kept for reuse); ids restart at 0. */
 ST_API st_status st_hists_clear(st_ctx* ctx);
 /* Queues n jobs at once (tracks[i] with descs[i]); job_ids may be NULL. */
@@ -222,6 +244,20 @@ typedef struct {
   int64_t done_ns;
 } st_completion;
 
+typedef struct {
+  int32_t batch, slot, n_jobs, status;
+  double units;              /* deposit x oversamples of the batch                           */
+  int64_t launch_ns;         /* steady clock: launch began, launch calls returned,           */
+  int64_t launched_ns;       /* predicted end of the fused kernel, completion handled        */
+  int64_t end_est_ns;
+  int64_t done_ns;
+  float prepare_ms, fused_ms;  /* device time of the prepare stage and of the fused kernel   */
+  float host_jobs_ms;          /* host time to queue the jobs and histograms of the batch    */
+  float host_run_ms;           /* host time of st_run_async (tables, uploads, launches)      */
+  int32_t grid;                /* CTAs of the fused launch                                   */
+  int32_t reserved;
+} st_batch_record;
+
 ST_API st_status st_server_create(int32_t device, int64_t budget_bytes, int64_t max_track_deposits,
                                   int32_t max_batch_jobs, st_server** out);
 ST_API st_status st_server_destroy(st_server* server);
@@ -243,6 +279,9 @@ ST_API st_status st_server_replay(st_server* server, int32_t n, const st_track_v
                                   int64_t* counts_out, double* yfy_out);
 /* Moves up to cap finished-job records into out; n_out receives the number moved. */
 ST_API st_status st_server_poll(st_server* server, st_completion* out, int32_t cap, int32_t* n_out);
+/* Moves up to cap records of finished batches into out; n_out receives the number moved. */
+ST_API st_status st_server_batches(st_server* server, st_batch_record* out, int32_t cap,
+                                   int32_t* n_out);
 /* Waits until every submitted (and replayed) job has completed, or timeout_ms elapses. */
 ST_API st_status st_server_drain(st_server* server, int64_t timeout_ms);
 

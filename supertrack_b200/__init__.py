@@ -224,6 +224,15 @@ class Context:
         self._check(lib().st_ctx_set_tuning(self._h, item_cost, grid), "st_ctx_set_tuning")
 
     # histograms ---------------------------------------------------------------------------
+    def set_param(self, name: str, value: int) -> None:
+        """Sets a named work-planning parameter (st_ctx_set_param)."""
+        self._check(lib().st_ctx_set_param(self._h, name.encode(), int(value)), "st_ctx_set_param")
+
+    def get_param(self, name: str) -> int:
+        v = C.c_int64(0)
+        self._check(lib().st_ctx_get_param(self._h, name.encode(), C.byref(v)), "st_ctx_get_param")
+        return v.value
+
     def histogram(self, kind: str, nbins: int, lower: float, upper: float) -> int:
         hid = C.c_int32(-1)
         self._check(lib().st_hist_create(self._h, HIST_TYPES[kind], nbins, lower, upper,
@@ -363,6 +372,13 @@ COMPLETION_DTYPE = np.dtype([("tag", "<u8"), ("status", "<i4"), ("batch", "<i4")
                              ("submit_ns", "<i8"), ("start_ns", "<i8"), ("done_ns", "<i8")])
 
 
+BATCH_DTYPE = np.dtype([("batch", "<i4"), ("slot", "<i4"), ("n_jobs", "<i4"), ("status", "<i4"),
+                        ("units", "<f8"), ("launch_ns", "<i8"), ("launched_ns", "<i8"),
+                        ("end_est_ns", "<i8"), ("done_ns", "<i8"), ("prepare_ms", "<f4"),
+                        ("fused_ms", "<f4"), ("host_jobs_ms", "<f4"), ("host_run_ms", "<f4"),
+                        ("grid", "<i4"), ("reserved", "<i4")])
+
+
 class Server:
     """Continuous-batching server (st_server_*): jobs on device-resident tracks are queued,
     admitted by device footprint against ``budget_bytes`` and run in batches on two alternating
@@ -462,6 +478,17 @@ class Server:
 
     def drain(self, timeout_s: float = 600.0) -> None:
         check(lib().st_server_drain(self._h, int(timeout_s * 1000)), "st_server_drain")
+
+    def batches(self, cap: int = 1 << 14) -> np.ndarray:
+        """Records of finished batches (each returned once)."""
+        out = np.zeros(cap, dtype=BATCH_DTYPE)
+        got = []
+        while True:
+            n = C.c_int32(0)
+            check(lib().st_server_batches(self._h, _ptr(out), cap, C.byref(n)), "st_server_batches")
+            got.append(out[: n.value].copy())
+            if n.value < cap:
+                return np.concatenate(got)
 
     def poll(self, cap: int = 1 << 16) -> np.ndarray:
         """Completion records of finished jobs (each returned once)."""

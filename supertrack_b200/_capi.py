@@ -105,6 +105,8 @@ SIGNATURES = [
     ("st_ctx_last_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                      C.POINTER(C.c_int32)]),
     ("st_ctx_set_tuning", C.c_int, [C.c_void_p, C.c_int64, C.c_int32]),
+    ("st_ctx_set_param", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
+    ("st_ctx_get_param", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
     ("st_hist_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_float,
                                  C.POINTER(C.c_int32)]),
     ("st_hist_read", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
@@ -128,7 +130,9 @@ SIGNATURES = [
     ("st_run_query", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("st_run_finish", C.c_int, [C.c_void_p]),
     ("st_hists_clear", C.c_int, [C.c_void_p]),
-    ("st_hist_read_all_async", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    ("st_hist_read_bins_async", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                                          C.c_void_p]),
+    ("st_ctx_order_after", C.c_int, [C.c_void_p, C.c_void_p]),
     ("st_server_create", C.c_int, [C.c_int32, C.c_int64, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_void_p)]),
     ("st_server_destroy", C.c_int, [C.c_void_p]),
@@ -143,6 +147,7 @@ SIGNATURES = [
                                    C.c_void_p]),
     ("st_server_poll", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     ("st_server_drain", C.c_int, [C.c_void_p, C.c_int64]),
+    ("st_server_batches", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     ("st_superimpose_noalloc", C.c_int, [C.POINTER(st_track_view), C.POINTER(st_job_desc),
                                          C.c_int32, C.c_int32, C.c_float, C.c_float,
                                          C.c_void_p, C.c_void_p, C.c_void_p,

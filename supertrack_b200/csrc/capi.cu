@@ -110,7 +110,10 @@ struct st_ctx {
   int64_t h_bins = 0, h_edge_total = 0;
 
   bool timing = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // run events: 0 start, 1 prepare and plan done, 4 fused start (after any cross-context wait),
+  // 2 fused done, 3 results copied to the host
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t order_after = nullptr;  // the next run's fused kernel waits for this event
   float t_prep = 0, t_fused = 0;
   int32_t launches = 0;
 
@@ -136,6 +139,9 @@ struct st_ctx {
   st::PlanParams cache_plan{};
   int chunk_windows = 4;      // windows (4096 deposits each) per chunk of a shared unit
   int max_helpers = 32;       // helper items per shared unit
+  int64_t spill_budget = 0;   // bytes for the spill tables; 0: 30% of free memory, at most 48 GB
+  int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
+  int min_chunks = 4;         // ... and kept > min_chunks chunks
 
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
@@ -347,15 +353,19 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(cudaMemcpyAsync(c->d_blk.p, blk.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
 
   // spill tables: one per resident CTA, able to hold every distinct sphere of the largest job;
-  // the number of resident CTAs shrinks if the tables would exceed 30% of free memory
+  // the number of resident CTAs shrinks if the tables would exceed the spill budget (by default
+  // 30% of free memory, at most 48 GB)
   int grid = c->grid_override > 0 ? c->grid_override : c->sm_count;
-  grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, work_jobs * std::max(1, c->max_helpers)));
+  // never more CTAs than work items can exist (every oversample as a shared unit with the
+  // most helpers)
+  grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, item_cap));
   const uint32_t gcap = std::max(c->gcap, next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024)));
   {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const size_t have = (size_t)c->gcap * (size_t)c->ggrid * 28;
-    const double budget = std::min(0.3 * (double)(free_b + have), 48e9);
+    const double budget = c->spill_budget > 0 ? (double)c->spill_budget
+                                              : std::min(0.3 * (double)(free_b + have), 48e9);
     const int fit = (int)std::max(1.0, std::floor(budget / ((double)gcap * 28.0)));
     grid = std::min(grid, fit);
   }
@@ -434,6 +444,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   q.max_helpers = c->max_helpers;
   q.grid = std::max(1, grid);
   q.item_cost = c->item_cost;
+  q.share_divisor = c->share_divisor;
+  q.min_chunks = c->min_chunks;
   q.total_units = (unsigned long long*)m;
   q.n_items = (int*)(m + 8);
   q.unit_counter = (unsigned int*)(m + 12);
@@ -490,21 +502,27 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
     fp.export_cap = (unsigned long long)ex_cap;
   }
 
-  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
+  ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
   ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->cache_any_flagged, c->stream), "prepare launch");
   ST_CUDA(st::launch_plan(c->cache_plan, c->stream), "plan launch");
-  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+  ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+  if (c->order_after) {
+    ST_CUDA(cudaStreamWaitEvent(c->stream, c->order_after, 0), "order after");
+    c->order_after = nullptr;
+  }
+  ST_CUDA(cudaEventRecord(c->ev[4], c->stream), "event");
   ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->stream), "fused launch");
-  if (c->timing) ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
+  ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
   c->launches += (c->cache_blocks > 0 ? 1 : 0) + (c->cache_grid > 0 ? 1 : 0);
 
   // ---- results into pinned host buffers
   if (c->h_aux_cap < nj) {
+    const size_t cap = std::max<size_t>(std::max<size_t>(nj, 1024), c->h_aux_cap + c->h_aux_cap / 2);
     if (c->h_aux) cudaFreeHost(c->h_aux);
     c->h_aux = nullptr;
     c->h_aux_cap = 0;
-    ST_CUDA(cudaMallocHost(&c->h_aux, std::max<size_t>(nj, 1024) * sizeof(JobAux)), "pinned aux");
-    c->h_aux_cap = std::max<size_t>(nj, 1024);
+    ST_CUDA(cudaMallocHost(&c->h_aux, cap * sizeof(JobAux)), "pinned aux");
+    c->h_aux_cap = cap;
   }
   if (!c->h_err) ST_CUDA(cudaMallocHost(&c->h_err, 32), "pinned flags");
   ST_CUDA(cudaMemcpyAsync(c->h_aux, c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
@@ -528,10 +546,10 @@ st_status finish_range(st_ctx* c, st_sphere* ex_out, int64_t ex_cap, int64_t* ex
   int errflags[4] = {c->h_err[0], c->h_err[1], c->h_err[2], c->h_err[3]};
   unsigned long long exn = 0;
   if (c->pend_export) std::memcpy(&exn, c->h_err + 4, 8);
-  if (c->timing) {
+  {
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
-    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&b, c->ev[4], c->ev[2]);
     c->t_prep += a;
     c->t_fused += b;
   }
@@ -748,6 +766,12 @@ st_status st_ctx_last_error(const st_ctx* c, char* buf, size_t len) {
 
 int32_t st_ctx_sm_count(const st_ctx* c) { return c ? c->sm_count : 0; }
 
+st_status st_ctx_order_after(st_ctx* c, const st_ctx* other) {
+  if (!c || !other || c == other) return ST_ERR_INVALID_ARGUMENT;
+  c->order_after = other->ev[2];
+  return ST_OK;
+}
+
 st_status st_ctx_enable_timing(st_ctx* c, int32_t on) {
   if (!c) return ST_ERR_INVALID_ARGUMENT;
   c->timing = on != 0;
@@ -766,6 +790,37 @@ st_status st_ctx_set_tuning(st_ctx* c, int64_t item_cost, int32_t grid) {
   if (!c || item_cost < 0 || grid < 0) return ST_ERR_INVALID_ARGUMENT;
   if (item_cost > 0) c->item_cost = item_cost;
   c->grid_override = grid;
+  return ST_OK;
+}
+
+st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
+  if (!c || !name) return ST_ERR_INVALID_ARGUMENT;
+  const std::string n(name);
+  if (n == "item_cost" && v >= 256 && v <= ((int64_t)1 << 40)) c->item_cost = v;
+  else if (n == "grid" && v >= 0 && v <= 1 << 20) c->grid_override = (int)v;
+  else if (n == "chunk_windows" && v >= 1 && v <= 1024) c->chunk_windows = (int)v;
+  else if (n == "max_helpers" && v >= 1 && v <= 4096) c->max_helpers = (int)v;
+  else if (n == "share_divisor" && v >= 0 && v <= 1 << 20) c->share_divisor = (int)v;
+  else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
+  else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
+  else return ST_ERR_INVALID_ARGUMENT;
+  c->cache_valid = false;
+  return ST_OK;
+}
+
+st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
+  if (!c || !name || !v) return ST_ERR_INVALID_ARGUMENT;
+  const std::string n(name);
+  if (n == "item_cost") *v = c->item_cost;
+  else if (n == "grid") *v = c->grid_override;
+  else if (n == "chunk_windows") *v = c->chunk_windows;
+  else if (n == "max_helpers") *v = c->max_helpers;
+  else if (n == "share_divisor") *v = c->share_divisor;
+  else if (n == "shared_min_chunks") *v = c->min_chunks;
+  else if (n == "spill_budget_bytes") *v = c->spill_budget;
+  else if (n == "last_grid") *v = c->cache_grid;       // read-only: CTAs of the last fused launch
+  else if (n == "spill_slots") *v = (int64_t)c->gcap;  // read-only: slots per spill table
+  else return ST_ERR_INVALID_ARGUMENT;
   return ST_OK;
 }
 
@@ -834,13 +889,13 @@ st_status st_hist_offset(const st_ctx* c, int32_t hist_id, int64_t* first_bin) {
   return ST_OK;
 }
 
-st_status st_hist_read_all_async(st_ctx* c, int64_t* counts, double* yfy, int64_t cap) {
-  if (!c) return ST_ERR_INVALID_ARGUMENT;
-  if (cap < c->h_bins) return ST_ERR_CAPACITY;
-  if (c->h_bins == 0) return ST_OK;
+st_status st_hist_read_bins_async(st_ctx* c, int64_t first_bin, int64_t n_bins, int64_t* counts,
+                                  double* yfy) {
+  if (!c || first_bin < 0 || n_bins < 0 || first_bin + n_bins > c->h_bins) return ST_ERR_INVALID_ARGUMENT;
+  if (n_bins == 0) return ST_OK;
   cudaSetDevice(c->device);
-  if (counts) ST_CUDA(cudaMemcpyAsync(counts, c->h_counts.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
-  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, c->h_yfy.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  if (counts) ST_CUDA(cudaMemcpyAsync(counts, (unsigned long long*)c->h_counts.p + first_bin, (size_t)n_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, (double*)c->h_yfy.p + first_bin, (size_t)n_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
   // an enqueued run now completes only once the copies have landed
   if (c->pending) ST_CUDA(cudaEventRecord(c->ev[3], c->stream), "event");
   return ST_OK;

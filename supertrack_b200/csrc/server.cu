@@ -4,10 +4,16 @@
 // tracks (SuperTrackManager.cu:49-102). A server instead takes (track, geometry, oversamples,
 // histogram) jobs while earlier ones are on the GPU:
 //   - a worker thread owns two contexts, each with its own stream and device arenas;
-//   - whenever a context is idle and jobs are queued, the worker admits queued jobs in arrival
+//   - when a context is idle and jobs are queued, the worker admits queued jobs in arrival
 //     order while their device footprint fits the budget, and launches them as one batch
-//     (prepare, plan, fused kernel, histogram read-back) without waiting; the batch's kernels
-//     queue behind the other context's batch and take over its SMs as they drain;
+//     (prepare, plan, fused kernel, histogram read-back) without waiting. While the other
+//     context's batch runs, the launch waits until that batch is expected to end within the
+//     time a launch takes on the host (its duration is predicted from the measured device
+//     throughput of earlier batches), so that the batch collects every job that arrives
+//     meanwhile and the GPU still does not idle between batches. The new batch's prepare
+//     kernels may overlap the running batch, its fused kernel is ordered after the running
+//     one's (st_ctx_order_after): a persistent kernel that has not yet placed all its CTAs is
+//     never starved by the next batch;
 //   - a finished batch (polled with an event query) hands every job its own spectrum, copied
 //     from pinned staging into the caller's arrays, and a completion record with its times.
 // Every job's spectrum depends only on its own track, geometry, seed and track id (the fused
@@ -86,6 +92,11 @@ struct Slot {
   int32_t batch = -1;
   int64_t start_ns = 0;
   int64_t footprint = 0;
+  double units = 0;          // deposit x oversamples of the batch
+  int64_t launched_ns = 0;   // host time when the launch calls returned
+  int64_t host_phase_ns[2] = {0, 0};  // run launch began, run launch returned
+  int64_t end_est_ns = 0;    // predicted end of its fused kernel
+  int64_t read_bins = 0;     // histogram bins read back (the used prefix of the arena)
   int64_t* pin_counts = nullptr;
   double* pin_yfy = nullptr;
   int64_t pin_cap = 0;
@@ -106,9 +117,16 @@ struct st_server {
   std::condition_variable cv_done;  // jobs completed
   std::deque<ServedJob> queue;
   std::vector<st_completion> done;
+  std::vector<st_batch_record> batch_log;
   int64_t in_flight_bytes = 0;
   int64_t outstanding = 0;  // submitted or scheduled, not yet completed
   int32_t next_batch = 0;
+  int next_slot = 0;
+  // predictions for the launch policy: fused-kernel throughput (deposit x oversamples per ms),
+  // the prepare stage of a batch that starts on an idle GPU, and the host time of a launch
+  double rate_per_ms = 5e7;
+  double batch_fixed_ms = 0.5;
+  double launch_ms = 0.5;
   std::atomic<bool> stop{false};
   std::thread worker;
   std::vector<std::thread> replayers;
@@ -117,7 +135,7 @@ struct st_server {
                       float lower, float upper, const void* counts, const void* yfy,
                       int64_t* footprint) const;
   void run_worker();
-  void launch(Slot& s, std::vector<ServedJob>&& batch);
+  void launch(Slot& s, Slot& other, std::vector<ServedJob>&& batch);
   void complete(Slot& s, st_status run_status);
 };
 
@@ -144,14 +162,17 @@ st_status st_server::check_job(const st_track_view* t, const st_job_desc* d, int
 // Enqueues one batch on an idle context: jobs, one histogram each (reused from earlier batches
 // when the spec matches, all zeroed first), the asynchronous run and the read-back of every bin
 // into pinned staging behind it.
-void st_server::launch(Slot& s, std::vector<ServedJob>&& batch) {
+void st_server::launch(Slot& s, Slot& other, std::vector<ServedJob>&& batch) {
   s.jobs = std::move(batch);
   s.busy = true;
   s.start_ns = now_ns();
+  s.units = 0;
+  for (const ServedJob& J : s.jobs) s.units += (double)J.track.n * (double)J.desc.n_oversamples;
   {
     std::lock_guard<std::mutex> lk(mu);
     s.batch = next_batch++;
   }
+  s.launched_ns = 0;
   st_status st = st_jobs_clear(s.ctx);
   if (st == ST_OK) {
     int64_t total = 0;
@@ -177,7 +198,14 @@ void st_server::launch(Slot& s, std::vector<ServedJob>&& batch) {
   }
   if (st == ST_OK) {
     int64_t bins = 0;
-    st_hist_read_all(s.ctx, nullptr, nullptr, 0, &bins);
+    for (int32_t id : s.hist_of_job) {
+      int64_t off = 0;
+      int32_t nb = 0;
+      st_hist_offset(s.ctx, id, &off);
+      st_hist_nbins(s.ctx, id, &nb);
+      bins = std::max<int64_t>(bins, off + nb);
+    }
+    s.read_bins = bins;
     if (bins > s.pin_cap) {
       if (s.pin_counts) cudaFreeHost(s.pin_counts);
       if (s.pin_yfy) cudaFreeHost(s.pin_yfy);
@@ -191,9 +219,18 @@ void st_server::launch(Slot& s, std::vector<ServedJob>&& batch) {
       else
         s.pin_cap = cap;
     }
+    if (st == ST_OK && other.busy) st = st_ctx_order_after(s.ctx, other.ctx);
+    s.host_phase_ns[0] = now_ns();
     if (st == ST_OK) st = st_run_async(s.ctx);
-    if (st == ST_OK) st = st_hist_read_all_async(s.ctx, s.pin_counts, s.pin_yfy, s.pin_cap);
+    s.host_phase_ns[1] = now_ns();
+    if (st == ST_OK) st = st_hist_read_bins_async(s.ctx, 0, bins, s.pin_counts, s.pin_yfy);
   }
+  const int64_t t1 = now_ns();
+  s.launched_ns = t1;
+  launch_ms = 0.8 * launch_ms + 0.2 * (t1 - s.start_ns) * 1e-6;
+  const int64_t fused_start = other.busy ? std::max<int64_t>(t1, other.end_est_ns)
+                                         : t1 + (int64_t)(batch_fixed_ms * 1e6);
+  s.end_est_ns = fused_start + (int64_t)(s.units / rate_per_ms * 1e6);
   if (st != ST_OK) {
     st_run_finish(s.ctx);
     complete(s, st);
@@ -202,6 +239,34 @@ void st_server::launch(Slot& s, std::vector<ServedJob>&& batch) {
 
 // Hands every job of a finished batch its spectrum and completion record.
 void st_server::complete(Slot& s, st_status run_status) {
+  st_batch_record rec{};
+  rec.batch = s.batch;
+  rec.slot = (int32_t)(&s - slots);
+  rec.n_jobs = (int32_t)s.jobs.size();
+  rec.status = run_status;
+  rec.units = s.units;
+  rec.launch_ns = s.start_ns;
+  rec.launched_ns = s.launched_ns;
+  rec.end_est_ns = s.end_est_ns;
+  rec.host_jobs_ms = (float)((s.host_phase_ns[0] - s.start_ns) * 1e-6);
+  rec.host_run_ms = (float)((s.host_phase_ns[1] - s.host_phase_ns[0]) * 1e-6);
+  {
+    int64_t g = 0;
+    st_ctx_get_param(s.ctx, "last_grid", &g);
+    rec.grid = (int32_t)g;
+  }
+  st_ctx_last_timing(s.ctx, &rec.prepare_ms, &rec.fused_ms, nullptr);
+  if (run_status == ST_OK || run_status == ST_ERR_NONFINITE_EDEP) {
+    // the fused kernel's own time (its prepare stage may have shared the GPU with the batch
+    // before it, so only the fused time measures this batch)
+    float fused = 0;
+    st_ctx_last_timing(s.ctx, nullptr, &fused, nullptr);
+    const double dev_ms = (double)fused;
+    if (s.units > 0 && dev_ms > 0.05) {
+      const double r = s.units / dev_ms;
+      rate_per_ms = 0.7 * rate_per_ms + 0.3 * r;
+    }
+  }
   std::vector<st_completion> out(s.jobs.size());
   for (size_t i = 0; i < s.jobs.size(); ++i) {
     ServedJob& J = s.jobs[i];
@@ -225,8 +290,10 @@ void st_server::complete(Slot& s, st_status run_status) {
   }
   const int64_t t = now_ns();
   for (auto& c : out) c.done_ns = t;
+  rec.done_ns = t;
   {
     std::lock_guard<std::mutex> lk(mu);
+    batch_log.push_back(rec);
     in_flight_bytes -= s.footprint;
     outstanding -= (int64_t)s.jobs.size();
     done.insert(done.end(), out.begin(), out.end());
@@ -247,8 +314,14 @@ void st_server::run_worker() {
       if (fin || q != ST_OK) complete(s, q);
     }
     bool any_busy = slots[0].busy || slots[1].busy;
-    for (Slot& s : slots) {
-      if (s.busy) continue;
+    {
+      // batches alternate between the two contexts
+      const int k = next_slot;
+      Slot& s = slots[k];
+      Slot& other = slots[1 - k];
+      if (s.busy) goto wait;
+      // while the other batch runs, launch only once it is about to end
+      if (other.busy && now_ns() < other.end_est_ns - (int64_t)((launch_ms + 0.3) * 1e6)) goto wait;
       std::vector<ServedJob> batch;
       {
         std::lock_guard<std::mutex> lk(mu);
@@ -262,10 +335,12 @@ void st_server::run_worker() {
         in_flight_bytes += taken;
         s.footprint = taken;
       }
-      if (batch.empty()) continue;
-      launch(s, std::move(batch));
+      if (batch.empty()) goto wait;
+      launch(s, other, std::move(batch));
+      next_slot = 1 - k;
       any_busy = true;
     }
+  wait:
     std::unique_lock<std::mutex> lk(mu);
     if (stop && queue.empty() && !any_busy) break;
     if (any_busy) {
@@ -304,6 +379,7 @@ st_status st_server_create(int32_t device, int64_t budget_bytes, int64_t max_tra
       (int64_t)pow2_at_least((uint64_t)std::max<int64_t>(2 * pad256(max_track_deposits), 1024));
   const int32_t sms = st_ctx_sm_count(s->slots[0].ctx);
   s->reserve = 2 * slots_per_table * 28 * (int64_t)std::max(sms, 1);
+  for (Slot& sl : s->slots) st_ctx_set_param(sl.ctx, "spill_budget_bytes", s->reserve / 2);
   s->budget = budget_bytes - s->reserve;
   if (s->budget <= 0) {
     for (Slot& o : s->slots) st_ctx_destroy(o.ctx);
@@ -421,6 +497,16 @@ st_status st_server_poll(st_server* s, st_completion* out, int32_t cap, int32_t*
   const size_t k = std::min<size_t>((size_t)cap, s->done.size());
   std::copy(s->done.begin(), s->done.begin() + k, out);
   s->done.erase(s->done.begin(), s->done.begin() + k);
+  *n_out = (int32_t)k;
+  return ST_OK;
+}
+
+st_status st_server_batches(st_server* s, st_batch_record* out, int32_t cap, int32_t* n_out) {
+  if (!s || !n_out || cap < 0 || (cap > 0 && !out)) return ST_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const size_t k = std::min<size_t>((size_t)cap, s->batch_log.size());
+  std::copy(s->batch_log.begin(), s->batch_log.begin() + k, out);
+  s->batch_log.erase(s->batch_log.begin(), s->batch_log.begin() + k);
   *n_out = (int32_t)k;
   return ST_OK;
 }

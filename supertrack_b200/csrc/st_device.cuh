@@ -174,6 +174,8 @@ struct PlanParams {
   int32_t max_helpers;
   int32_t grid;
   long long item_cost;
+  int32_t share_divisor;             // a job is shared when kept > total / (share_divisor * grid)
+  int32_t min_chunks;                // ... and kept > min_chunks chunks; share_divisor 0: never
   unsigned long long* total_units;   // sum of kept * n_os
   unsigned int* bucket_count;        // kPlanBuckets
   unsigned int* bucket_start;        // kPlanBuckets

@@ -901,8 +901,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
 
 // ---------------------------------------------------------------------------------------------
 // Planner (after the prepare stage, before k_fused): work items from the kept deposit counts.
-// A job whose kept deposits per oversample exceed both four chunks and an eighth of one CTA's
-// share of the batch runs as shared units (one per oversample, `helpers` helper items each);
+// A job whose kept deposits per oversample exceed both min_chunks chunks (4) and 1/share_divisor
+// (1/8) of one CTA's share of the batch runs as shared units (one per oversample, `helpers` helper items each);
 // every other job runs as private items of about item_cost deposit*oversamples. Items are
 // bucketed by cost, largest first (longest-processing-time order at bucket granularity).
 // ---------------------------------------------------------------------------------------------
@@ -933,8 +933,9 @@ __global__ void k_plan_size(PlanParams q) {
   pl.blk_os = 1;
   if (kept > 0 && nos > 0 && !(q.aux[j].flags & kAuxNonfinite)) {
     const long long chunk = (long long)q.chunk_windows * kWindow;
-    const long long share = (long long)(*q.total_units / (unsigned long long)(8 * q.grid));
-    if (kept > 4 * chunk && kept > share) {
+    const long long share =
+        q.share_divisor > 0 ? (long long)(*q.total_units / ((unsigned long long)q.share_divisor * q.grid)) : 0;
+    if (q.share_divisor > 0 && kept > (long long)q.min_chunks * chunk && kept > share) {
       const long long chunks = (kept + chunk - 1) / chunk;
       const int helpers = (int)(chunks < q.max_helpers ? chunks : q.max_helpers);
       pl.blk_os = helpers;

@@ -30,6 +30,12 @@ def served_workload(device="cuda", n_jobs: int = 10000, seed: int = 4, size_scal
     w = W.config2(device=device, n_tracks=n_jobs, seed=seed, size_scale=size_scale,
                   max_size=max_size)
     w.name = "served-stream"
+    if str(device).startswith("cuda"):
+        import torch
+        # the generator's temporaries stay in torch's cache otherwise, and the server's contexts
+        # size their spill tables from the free device memory
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
     return w
 
 
