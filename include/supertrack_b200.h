@@ -159,8 +159,10 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to
  *                      hold every sphere of the batch's largest job); the grid shrinks to fit;
  *                      0 = 30% of free device memory, at most 48 GB          (default 0)
- * st_ctx_get_param also reads "last_grid" (CTAs of the last fused launch) and "spill_slots"
- * (slots of each CTA's spill table). */
+ * st_ctx_get_param also reads "last_grid" (CTAs of the last fused launch), "spill_slots"
+ * (slots of each CTA's spill table) and the host cost of the last launch in microseconds:
+ * "last_host_launch_us", "last_host_tables_us", "last_host_alloc_us" (with "last_host_allocs"
+ * allocations) and "last_host_meminfo_us". */
 ST_API st_status st_ctx_set_param(st_ctx* ctx, const char* name, int64_t value);
 ST_API st_status st_ctx_get_param(const st_ctx* ctx, const char* name, int64_t* value);
 
@@ -255,7 +257,9 @@ typedef struct {
   float host_jobs_ms;          /* host time to queue the jobs and histograms of the batch    */
   float host_run_ms;           /* host time of st_run_async (tables, uploads, launches)      */
   int32_t grid;                /* CTAs of the fused launch                                   */
-  int32_t reserved;
+  int32_t host_allocs;         /* device/pinned allocations made by the launch               */
+  float host_tables_ms;        /* ... of which building the tables                           */
+  float host_alloc_ms;         /* ... of which allocating                                    */
 } st_batch_record;
 
 ST_API st_status st_server_create(int32_t device, int64_t budget_bytes, int64_t max_track_deposits,

@@ -376,7 +376,8 @@ BATCH_DTYPE = np.dtype([("batch", "<i4"), ("slot", "<i4"), ("n_jobs", "<i4"), ("
                         ("units", "<f8"), ("launch_ns", "<i8"), ("launched_ns", "<i8"),
                         ("end_est_ns", "<i8"), ("done_ns", "<i8"), ("prepare_ms", "<f4"),
                         ("fused_ms", "<f4"), ("host_jobs_ms", "<f4"), ("host_run_ms", "<f4"),
-                        ("grid", "<i4"), ("reserved", "<i4")])
+                        ("grid", "<i4"), ("host_allocs", "<i4"), ("host_tables_ms", "<f4"),
+                        ("host_alloc_ms", "<f4")])
 
 
 class Server:

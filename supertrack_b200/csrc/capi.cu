@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -29,6 +30,15 @@ using st::JobAux;
 using st::JobDev;
 using st::WorkItem;
 
+// Host time spent allocating (and freeing) device and pinned memory in the calling thread,
+// reported per run through st_ctx_get_param.
+thread_local double g_alloc_us = 0;
+thread_local int64_t g_allocs = 0;
+
+double now_us() {
+  return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -41,6 +51,11 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return cudaSuccess;
   if (b.bytes > 0) bytes = std::max(bytes, b.bytes + b.bytes / 2);
+  const double t0 = now_us();
+  struct Tally {
+    double t0;
+    ~Tally() { g_alloc_us += now_us() - t0; ++g_allocs; }
+  } tally{t0};
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
@@ -49,6 +64,32 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
   b.bytes = bytes;
   return cudaSuccess;
 }
+
+// Page-locked host staging for the per-run tables: copies from pageable memory would make the
+// host wait until the stream reaches them, i.e. behind whatever the GPU runs before this stream's
+// work gets SMs. Grow-only (by half again), freed with the context.
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+cudaError_t ensure_pinned(PinnedBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return cudaSuccess;
+  const size_t cap = std::max(bytes, b.bytes + b.bytes / 2);
+  struct Tally {
+    double t0;
+    ~Tally() { g_alloc_us += now_us() - t0; ++g_allocs; }
+  } tally{now_us()};
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMallocHost(&b.p, cap);
+  if (e != cudaSuccess) { b.p = nullptr; return e; }
+  b.bytes = cap;
+  return cudaSuccess;
+}
+
+size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 void release(DevBuf& b) {
   if (b.p) cudaFree(b.p);
@@ -146,6 +187,12 @@ struct st_ctx {
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
   size_t h_aux_cap = 0;
+  PinnedBuf stage;                // job, histogram, prepare-block and aux tables of the run
+  // host time of the last launch (microseconds): whole launch, table building, allocations
+  // inside it (and their number), the free-memory query
+  double host_launch_us = 0, host_tables_us = 0, host_alloc_us = 0, host_meminfo_us = 0;
+  int64_t host_allocs = 0;
+  size_t stage_aux_off = 0;
   int* h_err = nullptr;           // 4 ints + export count (8 bytes)
   bool pending = false;
   size_t pend_first = 0, pend_last = 0;
@@ -347,10 +394,22 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(ensure(c->d_blk_off, (size_t)blk[nj] * 8), "prepare block offsets");
   ST_CUDA(ensure(c->d_counter, 16), "work counter");
   ST_CUDA(ensure(c->d_err, 16), "error flags");
-  ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, jd.data(), nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
-  if (!hd.empty())
-    ST_CUDA(cudaMemcpyAsync(c->d_hists.p, hd.data(), hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
-  ST_CUDA(cudaMemcpyAsync(c->d_blk.p, blk.data(), (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
+  {
+    // tables through pinned staging (the previous run's copies from it have completed)
+    const size_t o_hists = align256(nj * sizeof(JobDev));
+    const size_t o_blk = o_hists + align256(hd.size() * sizeof(HistDev));
+    const size_t o_aux = o_blk + align256((nj + 1) * 8);
+    ST_CUDA(ensure_pinned(c->stage, o_aux + align256(nj * sizeof(JobAux))), "pinned staging");
+    char* st_base = (char*)c->stage.p;
+    std::memcpy(st_base, jd.data(), nj * sizeof(JobDev));
+    if (!hd.empty()) std::memcpy(st_base + o_hists, hd.data(), hd.size() * sizeof(HistDev));
+    std::memcpy(st_base + o_blk, blk.data(), (nj + 1) * 8);
+    c->stage_aux_off = o_aux;
+    ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, st_base, nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
+    if (!hd.empty())
+      ST_CUDA(cudaMemcpyAsync(c->d_hists.p, st_base + o_hists, hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
+    ST_CUDA(cudaMemcpyAsync(c->d_blk.p, st_base + o_blk, (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
+  }
 
   // spill tables: one per resident CTA, able to hold every distinct sphere of the largest job;
   // the number of resident CTAs shrinks if the tables would exceed the spill budget (by default
@@ -360,9 +419,13 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   // most helpers)
   grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, item_cap));
   const uint32_t gcap = std::max(c->gcap, next_pow2((uint64_t)std::max<int64_t>(2 * max_pad, 1024)));
-  {
+  if (gcap > c->gcap || grid > c->ggrid) {
+    // the free-memory query waits for other streams' work, so it is made only when the
+    // tables have to grow
     size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
+    const double tm = now_us();
+    if (c->spill_budget <= 0) cudaMemGetInfo(&free_b, &total_b);
+    c->host_meminfo_us = now_us() - tm;
     const size_t have = (size_t)c->gcap * (size_t)c->ggrid * 28;
     const double budget = c->spill_budget > 0 ? (double)c->spill_budget
                                               : std::min(0.3 * (double)(free_b + have), 48e9);
@@ -465,17 +528,36 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
 // launch, and the copy of the job counters and error flags into pinned host buffers. Nothing
 // waits; finish_range picks the results up.
 st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, int64_t ex_cap) {
+  const double t_begin = now_us();
+  g_alloc_us = 0;
+  g_allocs = 0;
+  c->host_meminfo_us = 0;
+  struct Stamp {
+    st_ctx* c;
+    double t0;
+    ~Stamp() {
+      c->host_launch_us = now_us() - t0;
+      c->host_alloc_us = g_alloc_us;
+      c->host_allocs = g_allocs;
+    }
+  } stamp{c, t_begin};
   const size_t nj = last - first;
   const bool reuse = !want_export && c->cache_valid && c->cache_first == first && c->cache_last == last;
+  c->host_tables_us = 0;
   if (!reuse) {
     st_status s = build_tables(c, first, last, want_export);
+    c->host_tables_us = now_us() - t_begin;
     if (s != ST_OK) { c->cache_valid = false; return s; }
   }
   {
     st_status s = upload_host_tracks(c, first, last, c->cache_arena_total);
     if (s != ST_OK) return s;
   }
-  ST_CUDA(cudaMemcpyAsync(c->d_aux.p, c->cache_aux.data(), nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
+  {
+    JobAux* st_aux = (JobAux*)((char*)c->stage.p + c->stage_aux_off);
+    std::memcpy(st_aux, c->cache_aux.data(), nj * sizeof(JobAux));
+    ST_CUDA(cudaMemcpyAsync(c->d_aux.p, st_aux, nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
+  }
   ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
   if (c->cache_grid > 0)
     ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
@@ -739,6 +821,7 @@ st_status st_ctx_destroy(st_ctx* c) {
   for (auto& e : c->ev) if (e) cudaEventDestroy(e);
   if (c->h_aux) cudaFreeHost(c->h_aux);
   if (c->h_err) cudaFreeHost(c->h_err);
+  if (c->stage.p) cudaFreeHost(c->stage.p);
   if (c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return ST_OK;
@@ -819,6 +902,11 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "last_grid") *v = c->cache_grid;       // read-only: CTAs of the last fused launch
+  else if (n == "last_host_launch_us") *v = (int64_t)c->host_launch_us;
+  else if (n == "last_host_tables_us") *v = (int64_t)c->host_tables_us;
+  else if (n == "last_host_alloc_us") *v = (int64_t)c->host_alloc_us;
+  else if (n == "last_host_allocs") *v = c->host_allocs;
+  else if (n == "last_host_meminfo_us") *v = (int64_t)c->host_meminfo_us;
   else if (n == "spill_slots") *v = (int64_t)c->gcap;  // read-only: slots per spill table
   else return ST_ERR_INVALID_ARGUMENT;
   return ST_OK;

@@ -254,6 +254,12 @@ void st_server::complete(Slot& s, st_status run_status) {
     int64_t g = 0;
     st_ctx_get_param(s.ctx, "last_grid", &g);
     rec.grid = (int32_t)g;
+    st_ctx_get_param(s.ctx, "last_host_allocs", &g);
+    rec.host_allocs = (int32_t)g;
+    st_ctx_get_param(s.ctx, "last_host_tables_us", &g);
+    rec.host_tables_ms = (float)(g * 1e-3);
+    st_ctx_get_param(s.ctx, "last_host_alloc_us", &g);
+    rec.host_alloc_ms = (float)(g * 1e-3);
   }
   st_ctx_last_timing(s.ctx, &rec.prepare_ms, &rec.fused_ms, nullptr);
   if (run_status == ST_OK || run_status == ST_ERR_NONFINITE_EDEP) {
