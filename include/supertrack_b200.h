@@ -35,7 +35,8 @@ typedef enum {
   ST_ERR_STATE = 10,           /* call out of order (e.g. reading stats before st_run)       */
   ST_ERR_IO = 11,
   ST_ERR_CONFIG = 12,          /* unusable .ini macro                                        */
-  ST_ERR_NO_DEVICE = 13
+  ST_ERR_NO_DEVICE = 13,
+  ST_ERR_DEVICE_WAIT = 14      /* a bounded device-side wait expired; the run is incomplete */
 } st_status;
 
 typedef enum { ST_ZSHIFT_PLUS = 0, ST_ZSHIFT_MINUS = 1, ST_ZSHIFT_NONE = 2 } st_zshift_mode;
@@ -156,15 +157,35 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   share_divisor      a job runs as shared units (one per oversample) when its kept deposits
  *                      exceed batch units / (share_divisor * grid); 0 = never (default 8)
  *   shared_min_chunks  ... and exceed this many chunks                       (default 4)
+ *   table_slots        shared-memory sphere table: 0 = 8192 slots when every histogram has at
+ *                      most 700 bins, else 4096; 4096 = always 4096          (default 0)
+ *   graphs             1 = a rerun of the same jobs replays a CUDA graph of the whole run
+ *                      (captured at the first rerun); 0 = enqueue every call (default 1)
  *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to
  *                      hold every sphere of the batch's largest job); the grid shrinks to fit;
  *                      0 = 30% of free device memory, at most 48 GB          (default 0)
  * st_ctx_get_param also reads "last_grid" (CTAs of the last fused launch), "spill_slots"
- * (slots of each CTA's spill table) and the host cost of the last launch in microseconds:
+ * (slots of each CTA's spill table), "graph_launches" (runs replayed from a CUDA graph) and
+ * the host cost of the last launch in microseconds:
  * "last_host_launch_us", "last_host_tables_us", "last_host_alloc_us" (with "last_host_allocs"
  * allocations) and "last_host_meminfo_us". */
 ST_API st_status st_ctx_set_param(st_ctx* ctx, const char* name, int64_t value);
 ST_API st_status st_ctx_get_param(const st_ctx* ctx, const char* name, int64_t* value);
+
+/* Autotuner: picks item_cost, chunk_windows, max_helpers, share_divisor and table_slots for the
+ * context's queued jobs by timing them (coordinate descent, at most max_trials batched runs of
+ * all jobs, best of two each). Replaces the reference's SuggestedCudaBlocks/SuggestedCudaThreads
+ * keys (VoxelConstrainedSphereMethod.cu:27-28, Histogram.cu:37-38). Histograms and job states are
+ * as before the call;
+ * the chosen parameters stay set. */
+typedef struct {
+  double default_ms;           /* prepare + fused device time with the parameters on entry */
+  double best_ms;              /* ... with the chosen parameters                           */
+  int64_t item_cost;
+  int32_t chunk_windows, max_helpers, share_divisor, table_slots;
+  int32_t trials, reserved;
+} st_tune_result;
+ST_API st_status st_ctx_autotune(st_ctx* ctx, int32_t max_trials, st_tune_result* out);
 
 /* --- histograms (device accumulators) ------------------------------------------------------ */
 

@@ -233,6 +233,13 @@ class Context:
         self._check(lib().st_ctx_get_param(self._h, name.encode(), C.byref(v)), "st_ctx_get_param")
         return v.value
 
+    def autotune(self, max_trials: int = 32) -> Dict[str, float]:
+        """Times the queued jobs under candidate planning parameters and keeps the fastest
+        (st_ctx_autotune); histograms and job states are unchanged."""
+        r = _capi.st_tune_result()
+        self._check(lib().st_ctx_autotune(self._h, max_trials, C.byref(r)), "st_ctx_autotune")
+        return {f: getattr(r, f) for f, _ in _capi.st_tune_result._fields_ if f != "reserved"}
+
     def histogram(self, kind: str, nbins: int, lower: float, upper: float) -> int:
         hid = C.c_int32(-1)
         self._check(lib().st_hist_create(self._h, HIST_TYPES[kind], nbins, lower, upper,

@@ -17,7 +17,7 @@ STATUS_NAMES = {
     3: "ST_ERR_BAD_HISTOGRAM", 4: "ST_ERR_CUDA", 5: "ST_ERR_OUT_OF_MEMORY",
     6: "ST_ERR_CAPACITY", 7: "ST_ERR_NONFINITE_EDEP", 8: "ST_ERR_DEVICE_OVERFLOW",
     9: "ST_ERR_NOT_FOUND", 10: "ST_ERR_STATE", 11: "ST_ERR_IO", 12: "ST_ERR_CONFIG",
-    13: "ST_ERR_NO_DEVICE",
+    13: "ST_ERR_NO_DEVICE", 14: "ST_ERR_DEVICE_WAIT",
 }
 for _v, _n in STATUS_NAMES.items():
     globals()[_n] = _v
@@ -72,6 +72,13 @@ class st_completion(C.Structure):
                 ("submit_ns", C.c_int64), ("start_ns", C.c_int64), ("done_ns", C.c_int64)]
 
 
+class st_tune_result(C.Structure):
+    _fields_ = [("default_ms", C.c_double), ("best_ms", C.c_double), ("item_cost", C.c_int64),
+                ("chunk_windows", C.c_int32), ("max_helpers", C.c_int32),
+                ("share_divisor", C.c_int32), ("table_slots", C.c_int32), ("trials", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 class st_run_info(C.Structure):
     _fields_ = [("n_tracks", C.c_int64), ("n_oversamples", C.c_int64),
                 ("n_effective", C.c_int64), ("random_seed", C.c_int64),
@@ -107,6 +114,7 @@ SIGNATURES = [
     ("st_ctx_set_tuning", C.c_int, [C.c_void_p, C.c_int64, C.c_int32]),
     ("st_ctx_set_param", C.c_int, [C.c_void_p, C.c_char_p, C.c_int64]),
     ("st_ctx_get_param", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    ("st_ctx_autotune", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(st_tune_result)]),
     ("st_hist_create", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_float,
                                  C.POINTER(C.c_int32)]),
     ("st_hist_read", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),

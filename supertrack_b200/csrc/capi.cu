@@ -18,7 +18,7 @@ namespace st {
 cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_flagged,
                            cudaStream_t s);
 cudaError_t configure_fused();
-cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s);
+cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
 }  // namespace st
@@ -155,6 +155,14 @@ struct st_ctx {
   // 2 fused done, 3 results copied to the host
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t order_after = nullptr;  // the next run's fused kernel waits for this event
+  // CUDA graph of a whole run, captured at the first rerun of the same tables
+  bool use_graphs = true;
+  cudaGraphExec_t gexec = nullptr;
+  int64_t build_id = 0, gexec_build = -1;
+  const void* gexec_aux = nullptr;
+  const void* gexec_stage = nullptr;
+  int64_t graph_launches = 0;
+  int table_slots = 0;        // shared-memory sphere table: 0 automatic, 4096 or 8192
   float t_prep = 0, t_fused = 0;
   int32_t launches = 0;
 
@@ -262,6 +270,7 @@ st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena
 // [first, last) and the launch parameters; stores them in the context cache.
 st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   const size_t nj = last - first;
+  ++c->build_id;
   int64_t prep_total = 0, arena_total = 0, max_pad = 0;
   for (size_t j = first; j < last; ++j) {
     JobHost& J = c->jobs[j];
@@ -527,6 +536,88 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
 // Enqueues jobs [first, last) of the context: uploads, prepare and plan launches, the fused
 // launch, and the copy of the job counters and error flags into pinned host buffers. Nothing
 // waits; finish_range picks the results up.
+// Enqueues the device side of a run on the context's stream: the upload of the job counters,
+// the resets, prepare, plan and fused kernels, and the copies of counters and flags into pinned
+// host memory, with the run's events. While the stream is being captured into a CUDA graph the
+// events become event-record nodes.
+st_status enqueue_run(st_ctx* c, const st::FusedParams& fp, size_t nj, bool want_export,
+                      bool capturing) {
+  const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  JobAux* st_aux = (JobAux*)((char*)c->stage.p + c->stage_aux_off);
+  ST_CUDA(cudaMemcpyAsync(c->d_aux.p, st_aux, nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
+  ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
+  if (c->cache_grid > 0)
+    ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
+  ST_CUDA(cudaMemsetAsync(c->d_plan_misc.p, 0, 16 + 3 * 4 * st::kPlanBuckets, c->stream), "plan reset");
+  if (c->cache_units > 0) {
+    ST_CUDA(cudaMemsetAsync(c->u_next.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+    ST_CUDA(cudaMemsetAsync(c->u_done.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+    ST_CUDA(cudaMemsetAsync(c->u_table.p, 0xFF, (size_t)c->cache_units * 4, c->stream), "unit reset");
+  }
+  if (c->cache_cells > 0) {
+    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+  }
+  ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
+  if (want_export) ST_CUDA(cudaMemsetAsync(c->ex_count.p, 0, 16, c->stream), "export counter");
+
+  ST_CUDA(cudaEventRecordWithFlags(c->ev[0], c->stream, evf), "event");
+  ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->cache_any_flagged, c->stream), "prepare launch");
+  ST_CUDA(st::launch_plan(c->cache_plan, c->stream), "plan launch");
+  ST_CUDA(cudaEventRecordWithFlags(c->ev[1], c->stream, evf), "event");
+  if (c->order_after && !capturing) {
+    ST_CUDA(cudaStreamWaitEvent(c->stream, c->order_after, 0), "order after");
+    c->order_after = nullptr;
+  }
+  ST_CUDA(cudaEventRecordWithFlags(c->ev[4], c->stream, evf), "event");
+  ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->table_slots, c->stream), "fused launch");
+  ST_CUDA(cudaEventRecordWithFlags(c->ev[2], c->stream, evf), "event");
+  ST_CUDA(cudaMemcpyAsync(c->h_aux, c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
+  ST_CUDA(cudaMemcpyAsync(c->h_err, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
+  if (want_export) ST_CUDA(cudaMemcpyAsync(c->h_err + 4, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
+  ST_CUDA(cudaEventRecordWithFlags(c->ev[3], c->stream, evf), "event");
+  return ST_OK;
+}
+
+void drop_graph(st_ctx* c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+}
+
+// Captures enqueue_run into a CUDA graph (once per set of tables); false if capture is not
+// possible here, in which case the caller enqueues directly and graphs stay off.
+bool capture_run(st_ctx* c, const st::FusedParams& fp, size_t nj) {
+  drop_graph(c);
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    c->use_graphs = false;
+    return false;
+  }
+  const st_status s = enqueue_run(c, fp, nj, false, true);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  cudaGraphExec_t x = nullptr;
+  const bool ok = s == ST_OK && e == cudaSuccess && g &&
+                  cudaGraphInstantiate(&x, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    if (x) cudaGraphExecDestroy(x);
+    c->use_graphs = false;
+    return false;
+  }
+  c->gexec = x;
+  c->gexec_build = c->build_id;
+  c->gexec_aux = c->h_aux;
+  c->gexec_stage = c->stage.p;
+  return true;
+}
+
+// Enqueues jobs [first, last) of the context: tables (unless the same jobs ran last), uploads,
+// the prepare and plan launches, the fused launch, and the copy of the job counters and error
+// flags into pinned host buffers. A rerun of the same jobs replays a captured CUDA graph of all
+// of it. Nothing waits; finish_range picks the results up.
 st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, int64_t ex_cap) {
   const double t_begin = now_us();
   g_alloc_us = 0;
@@ -553,51 +644,16 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
     st_status s = upload_host_tracks(c, first, last, c->cache_arena_total);
     if (s != ST_OK) return s;
   }
-  {
-    JobAux* st_aux = (JobAux*)((char*)c->stage.p + c->stage_aux_off);
-    std::memcpy(st_aux, c->cache_aux.data(), nj * sizeof(JobAux));
-    ST_CUDA(cudaMemcpyAsync(c->d_aux.p, st_aux, nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
-  }
-  ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
-  if (c->cache_grid > 0)
-    ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
-  ST_CUDA(cudaMemsetAsync(c->d_plan_misc.p, 0, 16 + 3 * 4 * st::kPlanBuckets, c->stream), "plan reset");
-  if (c->cache_units > 0) {
-    ST_CUDA(cudaMemsetAsync(c->u_next.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
-    ST_CUDA(cudaMemsetAsync(c->u_done.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
-    ST_CUDA(cudaMemsetAsync(c->u_table.p, 0xFF, (size_t)c->cache_units * 4, c->stream), "unit reset");
-  }
-  if (c->cache_cells > 0) {
-    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
-  }
-  ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
+  std::memcpy((char*)c->stage.p + c->stage_aux_off, c->cache_aux.data(), nj * sizeof(JobAux));
 
   st::FusedParams fp = c->cache_fp;
   if (want_export) {
     ST_CUDA(ensure(c->ex_buf, (size_t)std::max<int64_t>(ex_cap, 1) * sizeof(st::SphereRecord)), "export buffer");
     ST_CUDA(ensure(c->ex_count, 16), "export counter");
-    ST_CUDA(cudaMemsetAsync(c->ex_count.p, 0, 16, c->stream), "export counter");
     fp.export_buf = (st::SphereRecord*)c->ex_buf.p;
     fp.export_count = (unsigned long long*)c->ex_count.p;
     fp.export_cap = (unsigned long long)ex_cap;
   }
-
-  ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
-  ST_CUDA(st::launch_prepare(c->cache_pp, c->cache_blocks, c->cache_any_flagged, c->stream), "prepare launch");
-  ST_CUDA(st::launch_plan(c->cache_plan, c->stream), "plan launch");
-  ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
-  if (c->order_after) {
-    ST_CUDA(cudaStreamWaitEvent(c->stream, c->order_after, 0), "order after");
-    c->order_after = nullptr;
-  }
-  ST_CUDA(cudaEventRecord(c->ev[4], c->stream), "event");
-  ST_CUDA(st::launch_fused(fp, c->cache_max_nbins, c->cache_grid, c->stream), "fused launch");
-  ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
-  c->launches += (c->cache_blocks > 0 ? 1 : 0) + (c->cache_grid > 0 ? 1 : 0);
-
-  // ---- results into pinned host buffers
   if (c->h_aux_cap < nj) {
     const size_t cap = std::max<size_t>(std::max<size_t>(nj, 1024), c->h_aux_cap + c->h_aux_cap / 2);
     if (c->h_aux) cudaFreeHost(c->h_aux);
@@ -607,10 +663,25 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
     c->h_aux_cap = cap;
   }
   if (!c->h_err) ST_CUDA(cudaMallocHost(&c->h_err, 32), "pinned flags");
-  ST_CUDA(cudaMemcpyAsync(c->h_aux, c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
-  ST_CUDA(cudaMemcpyAsync(c->h_err, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
-  if (want_export) ST_CUDA(cudaMemcpyAsync(c->h_err + 4, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
-  ST_CUDA(cudaEventRecord(c->ev[3], c->stream), "event");
+
+  const bool graph = reuse && c->use_graphs && !c->order_after;
+  bool launched = false;
+  if (graph) {
+    if (!c->gexec || c->gexec_build != c->build_id || c->gexec_aux != c->h_aux ||
+        c->gexec_stage != c->stage.p)
+      capture_run(c, fp, nj);
+    if (c->gexec) {
+      ST_CUDA(cudaGraphLaunch(c->gexec, c->stream), "graph launch");
+      launched = true;
+      ++c->graph_launches;
+    }
+  }
+  if (!launched) {
+    st_status s = enqueue_run(c, fp, nj, want_export, false);
+    if (s != ST_OK) return s;
+  }
+  c->launches += (c->cache_blocks > 0 ? (c->cache_any_flagged ? 5 : 4) : 0) +
+                 (nj > 0 ? 4 : 0) + (c->cache_grid > 0 ? 1 : 0);
   c->pending = true;
   c->pend_first = first;
   c->pend_last = last;
@@ -656,6 +727,13 @@ st_status finish_range(st_ctx* c, st_sphere* ex_out, int64_t ex_cap, int64_t* ex
     c->cache_valid = false;
     c->err = "spill table overflow";
     return ST_ERR_DEVICE_OVERFLOW;
+  }
+  if (errflags[0] & (4 | 8)) {
+    // a work item gave up (no free spill table, or a shared unit's table was never published)
+    c->g_dirty = true;
+    c->cache_valid = false;
+    c->err = (errflags[0] & 4) ? "spill-table pool exhausted" : "shared-unit table wait expired";
+    return ST_ERR_DEVICE_WAIT;
   }
   if (ex_out) {
     if ((errflags[0] & 2) || exn > (unsigned long long)ex_cap) {
@@ -717,6 +795,7 @@ const char* st_status_string(st_status s) {
     case ST_ERR_IO: return "I/O error";
     case ST_ERR_CONFIG: return "configuration error";
     case ST_ERR_NO_DEVICE: return "no CUDA device";
+    case ST_ERR_DEVICE_WAIT: return "device-side wait expired";
   }
   return "unknown status";
 }
@@ -817,6 +896,7 @@ st_status st_ctx_destroy(st_ctx* c) {
                     &c->pool, &c->d_plan, &c->d_plan_misc, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};
+  drop_graph(c);
   for (DevBuf* b : bufs) release(*b);
   for (auto& e : c->ev) if (e) cudaEventDestroy(e);
   if (c->h_aux) cudaFreeHost(c->h_aux);
@@ -886,6 +966,8 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "share_divisor" && v >= 0 && v <= 1 << 20) c->share_divisor = (int)v;
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
+  else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
+  else if (n == "graphs" && (v == 0 || v == 1)) { c->use_graphs = v != 0; drop_graph(c); }
   else return ST_ERR_INVALID_ARGUMENT;
   c->cache_valid = false;
   return ST_OK;
@@ -901,6 +983,9 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "share_divisor") *v = c->share_divisor;
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
+  else if (n == "table_slots") *v = c->table_slots;
+  else if (n == "graphs") *v = c->use_graphs ? 1 : 0;
+  else if (n == "graph_launches") *v = c->graph_launches;  // read-only: runs replayed from a graph
   else if (n == "last_grid") *v = c->cache_grid;       // read-only: CTAs of the last fused launch
   else if (n == "last_host_launch_us") *v = (int64_t)c->host_launch_us;
   else if (n == "last_host_tables_us") *v = (int64_t)c->host_tables_us;
@@ -909,6 +994,90 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "last_host_meminfo_us") *v = (int64_t)c->host_meminfo_us;
   else if (n == "spill_slots") *v = (int64_t)c->gcap;  // read-only: slots per spill table
   else return ST_ERR_INVALID_ARGUMENT;
+  return ST_OK;
+}
+
+// Work-planning autotuner: coordinate descent over the planning parameters on the context's
+// queued jobs, each candidate timed (prepare + fused device time, best of two runs). Results are
+// exact and order-free, so parameters change only the time. The histograms are saved before the
+// trials and restored after them.
+st_status st_ctx_autotune(st_ctx* c, int32_t max_trials, st_tune_result* out) {
+  if (!c || !out || max_trials < 1) return ST_ERR_INVALID_ARGUMENT;
+  if (c->jobs.empty()) return ST_ERR_STATE;
+  cudaSetDevice(c->device);
+  if (c->pending) {
+    const st_status s = finish_range(c, nullptr, 0, nullptr);
+    if (s != ST_OK && s != ST_ERR_NONFINITE_EDEP) return s;
+  }
+  DevBuf save_c, save_y;
+  const size_t hb = (size_t)c->h_bins * 8;
+  if (hb) {
+    ST_CUDA(ensure(save_c, hb), "autotune save");
+    ST_CUDA(ensure(save_y, hb), "autotune save");
+    ST_CUDA(cudaMemcpyAsync(save_c.p, c->h_counts.p, hb, cudaMemcpyDeviceToDevice, c->stream), "autotune save");
+    ST_CUDA(cudaMemcpyAsync(save_y.p, c->h_yfy.p, hb, cudaMemcpyDeviceToDevice, c->stream), "autotune save");
+  }
+  std::vector<char> ran(c->jobs.size());
+  for (size_t j = 0; j < c->jobs.size(); ++j) ran[j] = c->jobs[j].ran;
+  st_status fail = ST_OK;
+  auto trial = [&]() -> double {
+    double best = 1e300;
+    for (int rep = 0; rep < 2 && fail == ST_OK; ++rep) {
+      for (auto& j : c->jobs) j.ran = false;
+      c->t_prep = c->t_fused = 0;
+      const st_status s = run_range(c, 0, c->jobs.size(), nullptr, 0, nullptr);
+      if (s != ST_OK && s != ST_ERR_NONFINITE_EDEP) { fail = s; break; }
+      best = std::min(best, (double)c->t_prep + (double)c->t_fused);
+    }
+    return best;
+  };
+  struct Knob {
+    const char* name;
+    std::vector<int64_t> values;
+  };
+  const Knob knobs[] = {
+      {"item_cost", {1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}},
+      {"chunk_windows", {1, 2, 4, 8, 16}},
+      {"max_helpers", {8, 16, 32, 64, 148}},
+      {"share_divisor", {2, 4, 8, 16, 0}},
+      {"table_slots", {0, 4096}},
+  };
+  out->default_ms = trial();
+  double best = out->default_ms;
+  int trials = 1;
+  for (const Knob& k : knobs) {
+    int64_t cur = 0;
+    st_ctx_get_param(c, k.name, &cur);
+    for (int64_t v : k.values) {
+      if (v == cur || trials >= max_trials || fail != ST_OK) continue;
+      st_ctx_set_param(c, k.name, v);
+      const double t = trial();
+      ++trials;
+      if (fail == ST_OK && t < best * 0.99) {
+        best = t;
+        cur = v;
+      } else {
+        st_ctx_set_param(c, k.name, cur);
+      }
+    }
+  }
+  if (hb) {
+    ST_CUDA(cudaMemcpyAsync(c->h_counts.p, save_c.p, hb, cudaMemcpyDeviceToDevice, c->stream), "autotune restore");
+    ST_CUDA(cudaMemcpyAsync(c->h_yfy.p, save_y.p, hb, cudaMemcpyDeviceToDevice, c->stream), "autotune restore");
+    ST_CUDA(cudaStreamSynchronize(c->stream), "autotune restore");
+  }
+  release(save_c);
+  release(save_y);
+  for (size_t j = 0; j < c->jobs.size(); ++j) c->jobs[j].ran = ran[j] != 0;
+  if (fail != ST_OK) return fail;
+  out->best_ms = best;
+  out->item_cost = c->item_cost;
+  out->chunk_windows = c->chunk_windows;
+  out->max_helpers = c->max_helpers;
+  out->share_divisor = c->share_divisor;
+  out->table_slots = c->table_slots;
+  out->trials = trials;
+  out->reserved = 0;
   return ST_OK;
 }
 

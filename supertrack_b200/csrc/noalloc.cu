@@ -30,7 +30,7 @@ namespace st {
 cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_flagged,
                            cudaStream_t s);
 cudaError_t configure_fused();
-cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s);
+cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s);
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
 }  // namespace st
 
@@ -306,7 +306,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
 
   NA_CUDA(st::launch_prepare(pp, n_blocks, D.flagged != 0, st_));
   NA_CUDA(st::launch_plan(q, st_));
-  NA_CUDA(st::launch_fused(fp, nbins, kNaGrid, st_));
+  NA_CUDA(st::launch_fused(fp, nbins, kNaGrid, 0, st_));
 
   // ---- status: job counters and device error flags (host stack destinations)
   st::JobAux out;

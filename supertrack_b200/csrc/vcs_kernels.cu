@@ -1063,11 +1063,12 @@ cudaError_t configure_fused() {
                               (int)fused_smem_bytes(8192, kSmallHistBins));
 }
 
-// Picks the kernel shape from the largest histogram of the batch; fills P.smem_hist_bins and
-// P.flush_threshold.
-cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, cudaStream_t s) {
+// Picks the kernel shape: the 8192-slot sphere table when the largest histogram of the batch
+// fits the remaining shared memory (and table_slots does not ask for 4096), else 4096 slots with
+// room for 4096 bins; fills P.smem_hist_bins and P.flush_threshold.
+cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
-  if (max_nbins <= kSmallHistBins) {
+  if (max_nbins <= kSmallHistBins && table_slots != 4096) {
     p.smem_hist_bins = kSmallHistBins;
     p.flush_threshold = 8192 / 2;
     k_fused<8192, kFusedThreads>

@@ -1,0 +1,94 @@
+"""CUDA-graph reruns and the planning autotuner.
+
+A rerun of the same jobs replays a captured graph of the whole run; its results must equal the
+directly enqueued run's (counts bit-exact, y*f(y) within 1e-12). The autotuner times candidate
+planning parameters on the queued jobs; it must leave histograms and job states as they were, and
+the tuned parameters must give the same spectra as the defaults.
+"""
+import numpy as np
+import pytest
+
+import supertrack_b200 as st
+import supertrack_b200.workloads as W
+
+from helpers import assert_hist_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def _submit(c, w):
+    hs = [c.histogram(*h) for h in w.hists]
+    for j in range(w.n_jobs):
+        x, y, z, e = w.job_arrays(j)
+        c.submit(x, y, z, e, half_length=float(w.half_length[j]),
+                 sphere_diameter=float(w.diameter[j]), n_oversamples=int(w.n_os[j]),
+                 hist=hs[int(w.hist_of_job[j])], seed=int(w.seed[j]), track_id=int(w.track_id[j]),
+                 zshift=w.zshift, on_device=True)
+    return hs
+
+
+def _spectra(c, hs):
+    out = [c.read_histogram(h) for h in hs]
+    return [o[0] for o in out], [o[1] for o in out]
+
+
+@pytest.fixture(scope="module")
+def work():
+    return W.config2(device="cuda", n_tracks=96, seed=21, size_scale=0.2, max_size=300_000)
+
+
+def test_graph_rerun_equals_direct(work):
+    res = {}
+    for graphs in (0, 1):
+        with st.Context(0) as c:
+            c.set_param("graphs", graphs)
+            hs = _submit(c, work)
+            for _ in range(3):            # first run builds tables, reruns replay
+                c.jobs_reset()
+                c.run("batched")
+            res[graphs] = (_spectra(c, hs), [c.stats(j) for j in range(work.n_jobs)],
+                           c.get_param("graph_launches"))
+    (c0, y0), s0, g0 = res[0]
+    (c1, y1), s1, g1 = res[1]
+    assert g0 == 0 and g1 == 2
+    assert_hist_equal(c1, y1, c0, y0)
+    assert s0 == s1
+
+
+def test_autotune_keeps_state_and_results(work):
+    with st.Context(0) as c:
+        hs = _submit(c, work)
+        c.run("batched")
+        before = _spectra(c, hs)
+        stats = [c.stats(j) for j in range(work.n_jobs)]
+        r = c.autotune(max_trials=8)
+        assert r["trials"] <= 8 and r["best_ms"] <= r["default_ms"]
+        assert r["best_ms"] > 0
+        after = _spectra(c, hs)
+        assert_hist_equal(after[0], after[1], before[0], before[1], rtol=0)
+        assert [c.stats(j) for j in range(work.n_jobs)] == stats
+        # the jobs count as run: a new run needs a reset, and with the tuned parameters it
+        # adds exactly the same spectrum again
+        c.jobs_reset()
+        c.run("batched")
+        twice = _spectra(c, hs)
+        for a, b in zip(twice[0], before[0]):
+            assert np.array_equal(a, 2 * b)
+        for a, b in zip(twice[1], before[1]):
+            np.testing.assert_allclose(a, 2 * b, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("name,value", [("item_cost", 1 << 16), ("chunk_windows", 1),
+                                        ("max_helpers", 8), ("share_divisor", 0),
+                                        ("table_slots", 4096)])
+def test_planning_parameters_do_not_change_results(work, name, value):
+    res = []
+    for set_it in (False, True):
+        with st.Context(0) as c:
+            if set_it:
+                c.set_param(name, value)
+                assert c.get_param(name) == value
+            hs = _submit(c, work)
+            c.run("batched")
+            res.append(_spectra(c, hs))
+    assert_hist_equal(res[1][0], res[1][1], res[0][0], res[0][1])
