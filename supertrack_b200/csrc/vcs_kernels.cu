@@ -60,15 +60,23 @@ __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y
   return fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
 }
 
-// Cell of side cell_size (slightly above d) containing (x, y, z), offset by (dx, dy, dz) cells.
-// Two deposits within distance d of each other lie in the same or in adjacent cells.
-__device__ __forceinline__ uint64_t cell_key(double x, double y, double z, double cs, int dx,
-                                             int dy, int dz) {
+// Cell of side cell_size (slightly above d) containing (x, y, z): integer cell coordinates,
+// offset to be non-negative. Two deposits within distance d of each other lie in the same or in
+// adjacent cells.
+struct CellCoord {
+  long long x, y, z;
+};
+
+__device__ __forceinline__ CellCoord cell_of(double x, double y, double z, double cs) {
   const long long off = 1ll << (kCellBits - 1);
-  const uint64_t cx = (uint64_t)((long long)floor(__ddiv_rn(x, cs)) + off + dx);
-  const uint64_t cy = (uint64_t)((long long)floor(__ddiv_rn(y, cs)) + off + dy);
-  const uint64_t cz = (uint64_t)((long long)floor(__ddiv_rn(z, cs)) + off + dz);
-  return (cz << (2 * kCellBits)) | (cy << kCellBits) | cx;
+  return {(long long)floor(__ddiv_rn(x, cs)) + off, (long long)floor(__ddiv_rn(y, cs)) + off,
+          (long long)floor(__ddiv_rn(z, cs)) + off};
+}
+
+// Key of the cell at offset (dx, dy, dz) from c.
+__device__ __forceinline__ uint64_t cell_key(const CellCoord& c, int dx, int dy, int dz) {
+  return ((uint64_t)(c.z + dz) << (2 * kCellBits)) | ((uint64_t)(c.y + dy) << kCellBits) |
+         (uint64_t)(c.x + dx);
 }
 
 __device__ __forceinline__ void cell_insert(const PrepareParams& p, const JobDev& J,
@@ -238,7 +246,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (J.flagged) {
         p.PZ[dst] = z1;
-        cell_insert(p, J, cell_key(x, y, z1, J.cell_size, 0, 0, 0), (uint32_t)(k / kWindow));
+        cell_insert(p, J, cell_key(cell_of(x, y, z1, J.cell_size), 0, 0, 0), (uint32_t)(k / kWindow));
       }
     }
     run += total;
@@ -283,9 +291,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
     const double x = p.PX[dst], y = p.PY[dst], z = p.PZ[dst];
     const uint32_t win = (uint32_t)(k / kWindow);
+    const CellCoord cc = cell_of(x, y, z, J.cell_size);
     bool boundary = false;
     for (int c = 0; c < 27 && !boundary; ++c)
-      boundary = cell_foreign(p, J, cell_key(x, y, z, J.cell_size, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win);
+      boundary = cell_foreign(p, J, cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win);
     if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
 }
