@@ -369,6 +369,21 @@ ST_API float st_ini_get_float(const st_ini* ini, const char* section, const char
 ST_API int32_t st_ini_get_boolean(const st_ini* ini, const char* section, const char* name,
                                   int32_t dflt);
 
+/* --- spectrum post-processing (host; CPUHistogramUtils, utils.cc:37-117) --------------------
+ * `contents` uses ROOT's TH1 layout: nbins + 2 values, [0] underflow, [1..nbins] the bins
+ * (st_hist_read's bin b is contents[b + 1]), [nbins + 1] overflow; `edges` has nbins + 1 values.
+ * The reference's loops cover indices 0..nbins-1 (the underflow bin, with ROOT's equidistant low
+ * edge below the axis, and every bin but the last) and sum the normalisation in float; these
+ * functions do the same, so they return the reference's numbers. */
+/* BinLogX (utils.cc:37-57): edges 10^(from + i*(to - from)/nbins), i = 0..nbins. */
+ST_API st_status st_spectrum_bin_log_x(int32_t nbins, double from_log10, double to_log10,
+                                       double* edges);
+/* PMF_to_PDF (utils.cc:81-102): divide by bin width, then by the sum of the original contents. */
+ST_API st_status st_spectrum_pmf_to_pdf(int32_t nbins, const double* edges, double* contents);
+/* Prepare_for_Semilog (utils.cc:104-117): multiply by the bin midpoint (f(y) -> y*f(y)). */
+ST_API st_status st_spectrum_prepare_for_semilog(int32_t nbins, const double* edges,
+                                                 double* contents);
+
 /* Task list of a macro: ThreadAllocator::ReturnThreadAllocations (ThreadAllocator.cc:51-109)
  * flattened; per task: thread id, entry/exit points, task seed, file ordinal (1-based). */
 typedef struct {

@@ -163,3 +163,52 @@ def run_batch(x, y, z, edep, off, n, hl, d, zshift, shift_track, n_os, seed, tra
         raise RuntimeError(f"{failed} oracle jobs failed")
     return ([counts[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))],
             [yfy[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))])
+
+
+# ---------------------------------------------------------------------------------------------
+# Spectrum post-processing, restated from utils.cc:37-117 (CPUHistogramUtils) for ROOT-layout
+# contents (index 0 underflow, 1..nbins bins, nbins+1 overflow). TAxis::GetBinLowEdge of an
+# axis built from explicit edges returns edges[bin-1] for bins 1..nbins+1 and extrapolates with
+# the mean width outside. The normalisation accumulates in float (float_t) as in the reference.
+# ---------------------------------------------------------------------------------------------
+def _root_low_edge(edges, bin_):
+    nb = len(edges) - 1
+    if bin_ < 1 or bin_ > nb + 1:
+        w = (float(edges[nb]) - float(edges[0])) / nb
+        return float(edges[0]) + (bin_ - 1) * w
+    return float(edges[bin_ - 1])
+
+
+def bin_log_x(nbins, frm, to):
+    """utils.cc:37-57: 10^(from + i*width), width = (to - from) / nbins."""
+    width = (frm * 0 + to - frm) / nbins
+    return np.array([10.0 ** (frm + i * width) for i in range(nbins + 1)])
+
+
+def pmf_to_pdf(edges, contents):
+    """utils.cc:81-102: loops over indices 0..nbins-1; float normalisation."""
+    c = [float(v) for v in contents]
+    nb = len(edges) - 1
+    norm = np.float32(0.0)
+    for i in range(nb):
+        value = c[i]
+        low = _root_low_edge(edges, i)
+        high = _root_low_edge(edges, i + 1)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            c[i] = float(np.float64(value) / np.float64(high - low))
+        norm = np.float32(float(norm) + value)
+    with np.errstate(divide="ignore", invalid="ignore"):   # IEEE division, as in C++
+        for i in range(nb):
+            c[i] = float(np.float64(c[i]) / np.float64(float(norm)))
+    return np.array(c)
+
+
+def prepare_for_semilog(edges, contents):
+    """utils.cc:104-117: multiplies indices 0..nbins-1 by their bin midpoints."""
+    c = [float(v) for v in contents]
+    nb = len(edges) - 1
+    for i in range(nb):
+        low = _root_low_edge(edges, i)
+        high = _root_low_edge(edges, i + 1)
+        c[i] = c[i] * ((high + low) / 2)
+    return np.array(c)

@@ -23,7 +23,7 @@ __all__ = [
     "StError", "Context", "geometry", "hist_edges", "philox4x32_10", "oversample_shifts",
     "INIReader", "SphericalGeometry", "Histogram", "VoxelConstrainedSphereMethod",
     "SuperTrackManager", "run_macro", "macro_tasks", "write_track_file", "ZSHIFT",
-    "HIST_TYPES", "Server",
+    "HIST_TYPES", "Server", "CPUHistogramUtils", "to_root_layout",
 ]
 
 ZSHIFT = {"plus": ST_ZSHIFT_PLUS, "minus": ST_ZSHIFT_MINUS, "none": ST_ZSHIFT_NONE}
@@ -76,6 +76,48 @@ def oversample_shifts(half_length: float, sphere_diameter: float, shift_track: b
     check(lib().st_oversample_shifts(C.byref(g), int(bool(shift_track)), seed, track_id,
                                      os_begin, n_os, _ptr(out)), "st_oversample_shifts")
     return out.reshape(-1, 2)
+
+
+class CPUHistogramUtils:
+    """Spectrum post-processing of the reference (utils.cc:37-117) on ROOT-layout contents:
+    nbins + 2 float64 values, [0] underflow, [1..nbins] the bins, [nbins + 1] overflow (see
+    :func:`to_root_layout`). Like the reference's loops, PMF_to_PDF and Prepare_for_Semilog touch
+    indices 0..nbins-1 only (the underflow bin and every bin but the last) and sum the
+    normalisation in float, so they return the reference's numbers."""
+
+    @staticmethod
+    def BinLogX(nbins: int, from_log10: float, to_log10: float) -> np.ndarray:
+        e = np.zeros(nbins + 1)
+        check(lib().st_spectrum_bin_log_x(nbins, from_log10, to_log10, _ptr(e)),
+              "st_spectrum_bin_log_x")
+        return e
+
+    @staticmethod
+    def PMF_to_PDF(edges: np.ndarray, contents: np.ndarray) -> np.ndarray:
+        e = np.ascontiguousarray(edges, dtype=np.float64)
+        c = np.array(contents, dtype=np.float64)
+        if len(c) != len(e) + 1:
+            raise ValueError("contents must have nbins + 2 values (ROOT layout)")
+        check(lib().st_spectrum_pmf_to_pdf(len(e) - 1, _ptr(e), _ptr(c)), "st_spectrum_pmf_to_pdf")
+        return c
+
+    @staticmethod
+    def Prepare_for_Semilog(edges: np.ndarray, contents: np.ndarray) -> np.ndarray:
+        e = np.ascontiguousarray(edges, dtype=np.float64)
+        c = np.array(contents, dtype=np.float64)
+        if len(c) != len(e) + 1:
+            raise ValueError("contents must have nbins + 2 values (ROOT layout)")
+        check(lib().st_spectrum_prepare_for_semilog(len(e) - 1, _ptr(e), _ptr(c)),
+              "st_spectrum_prepare_for_semilog")
+        return c
+
+
+def to_root_layout(counts: np.ndarray) -> np.ndarray:
+    """Bin contents (st_hist_read order) as a ROOT TH1 array with empty under/overflow bins,
+    as Histogram::AccumulateCPUHistogram fills them (Histogram.cu:177-186)."""
+    c = np.zeros(len(counts) + 2)
+    c[1:-1] = counts
+    return c
 
 
 def write_track_file(path: str, tracks: Sequence[Tuple[np.ndarray, np.ndarray, np.ndarray,

@@ -174,6 +174,9 @@ SIGNATURES = [
     ("st_ini_get_real", C.c_double, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double]),
     ("st_ini_get_float", C.c_float, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_float]),
     ("st_ini_get_boolean", C.c_int32, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int32]),
+    ("st_spectrum_bin_log_x", C.c_int, [C.c_int32, C.c_double, C.c_double, C.c_void_p]),
+    ("st_spectrum_pmf_to_pdf", C.c_int, [C.c_int32, C.c_void_p, C.c_void_p]),
+    ("st_spectrum_prepare_for_semilog", C.c_int, [C.c_int32, C.c_void_p, C.c_void_p]),
     ("st_macro_tasks", C.c_int, [C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64),
                                  C.c_char_p, C.c_size_t]),
 ]

@@ -360,4 +360,46 @@ bool WriteTrackFile(const std::string& path, uint64_t n_tracks, const uint64_t* 
   return ok;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Spectrum post-processing (utils.cc:37-117)
+// ---------------------------------------------------------------------------------------------
+namespace CPUHistogramUtils {
+namespace {
+// TAxis::GetBinLowEdge of an axis built from explicit edges: the edge for bins 1..nbins+1,
+// the equidistant extrapolation below (or above) that range.
+double low_edge(int nbins, const double* edges, int bin) {
+  if (bin < 1 || bin > nbins + 1) {
+    const double w = (edges[nbins] - edges[0]) / (double)nbins;
+    return edges[0] + (double)(bin - 1) * w;
+  }
+  return edges[bin - 1];
+}
+}  // namespace
+
+void BinLogX(int nbins, double from, double to, double* edges) {
+  const double width = (to - from) / nbins;
+  for (int i = 0; i <= nbins; i++) edges[i] = std::pow(10.0, from + i * width);
+}
+
+void PMF_to_PDF(int nbins, const double* edges, double* contents) {
+  float normalization = 0;
+  for (int i = 0; i < nbins; i++) {
+    const double value = contents[i];
+    const double low = low_edge(nbins, edges, i);
+    const double high = low_edge(nbins, edges, i + 1);
+    contents[i] = value / (high - low);
+    normalization += value;
+  }
+  for (int i = 0; i < nbins; i++) contents[i] = contents[i] / normalization;
+}
+
+void Prepare_for_Semilog(int nbins, const double* edges, double* contents) {
+  for (int i = 0; i < nbins; i++) {
+    const double low = low_edge(nbins, edges, i);
+    const double high = low_edge(nbins, edges, i + 1);
+    contents[i] = contents[i] * ((high + low) / 2);
+  }
+}
+}  // namespace CPUHistogramUtils
+
 }  // namespace st

@@ -54,6 +54,23 @@ void LogSpace(float bottom, float top, int nbins, double* bins);
 bool MakeEdges(int type, int nbins, float lower, float upper, std::vector<double>* edges);
 
 // ---------------------------------------------------------------------------------------------
+// Spectrum post-processing (CPUHistogramUtils, utils.cc:37-117). The reference applies these to
+// a ROOT TH1 built with the bin edges, whose contents are indexed like ROOT's: 0 is the
+// underflow bin, 1..nbins the bins, nbins+1 the overflow bin. `contents` has that layout here
+// (nbins + 2 values). The reference's loops run over indices 0..nbins-1, so they touch the
+// underflow bin (with ROOT's equidistant low edge below the axis) and leave the last bin alone;
+// its normalisation sum is a float. Both are kept, so the outputs equal the reference's.
+// ---------------------------------------------------------------------------------------------
+namespace CPUHistogramUtils {
+// Edges of an axis given in log10 units: 10^(from + i * (to - from) / nbins), i = 0..nbins.
+void BinLogX(int nbins, double from, double to, double* edges);
+// Counts per bin to a normalised density (divide by bin width, then by the count total).
+void PMF_to_PDF(int nbins, const double* edges, double* contents);
+// Density to y*f(y) (multiply by the bin midpoint).
+void Prepare_for_Semilog(int nbins, const double* edges, double* contents);
+}  // namespace CPUHistogramUtils
+
+// ---------------------------------------------------------------------------------------------
 // Tasks and their seeds (ThreadTask.hh:6-31, ThreadAllocation.cc:16-32, ThreadAllocator.cc).
 // ---------------------------------------------------------------------------------------------
 struct ThreadTask {

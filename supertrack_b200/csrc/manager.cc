@@ -448,4 +448,22 @@ int32_t st_ini_get_boolean(const st_ini* ini, const char* s, const char* n, int3
   return ini ? (ini->r.GetBoolean(s, n, d != 0) ? 1 : 0) : d;
 }
 
+st_status st_spectrum_bin_log_x(int32_t nbins, double from_log10, double to_log10, double* edges) {
+  if (nbins < 1 || !edges) return ST_ERR_INVALID_ARGUMENT;
+  st::CPUHistogramUtils::BinLogX(nbins, from_log10, to_log10, edges);
+  return ST_OK;
+}
+
+st_status st_spectrum_pmf_to_pdf(int32_t nbins, const double* edges, double* contents) {
+  if (nbins < 1 || !edges || !contents) return ST_ERR_INVALID_ARGUMENT;
+  st::CPUHistogramUtils::PMF_to_PDF(nbins, edges, contents);
+  return ST_OK;
+}
+
+st_status st_spectrum_prepare_for_semilog(int32_t nbins, const double* edges, double* contents) {
+  if (nbins < 1 || !edges || !contents) return ST_ERR_INVALID_ARGUMENT;
+  st::CPUHistogramUtils::Prepare_for_Semilog(nbins, edges, contents);
+  return ST_OK;
+}
+
 }  // extern "C"

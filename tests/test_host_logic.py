@@ -343,3 +343,38 @@ def test_server_job_footprint():
     # 1e5 deposits: flagged for d = 10 nm (N = 500), not for d = 1000 nm (N = 5)
     assert foot(100_000, d=10.0)[1] - foot(100_000, d=1000.0)[1] >= 16 * 2 * 100_000
     assert foot(1000, d=-1.0)[0] == _capi.ST_ERR_BAD_GEOMETRY
+
+
+@pytest.mark.parametrize("kind,nb,lo,hi", [("log", 200, 0.01, 1e4), ("lin", 3000, 0.01, 300.0),
+                                          ("log", 7, 0.5, 2.0), ("lin", 1, 0.0, 1.0)])
+def test_spectrum_post_processing_matches_oracle(kind, nb, lo, hi):
+    """PMF_to_PDF and Prepare_for_Semilog (utils.cc:81-117) on ROOT-layout contents: bit-equal
+    to the oracle's restatement, including the reference's index range (underflow bin in, last
+    bin untouched) and its float normalisation."""
+    rs = np.random.default_rng(nb)
+    edges = po.edges(kind, nb, lo, hi)
+    counts = rs.integers(0, 10_000, nb).astype(np.float64)
+    c = st.to_root_layout(counts)
+    assert c[0] == 0 and c[-1] == 0 and np.array_equal(c[1:-1], counts)
+    pdf = st.CPUHistogramUtils.PMF_to_PDF(edges, c)
+    assert np.array_equal(pdf, po.pmf_to_pdf(edges, c), equal_nan=True)
+    semi = st.CPUHistogramUtils.Prepare_for_Semilog(edges, pdf)
+    assert np.array_equal(semi, po.prepare_for_semilog(edges, pdf), equal_nan=True)
+    # the last bin keeps its raw count in both steps (the reference's loops stop before it)
+    assert pdf[nb] == counts[-1] and semi[nb] == counts[-1]
+    if nb > 1:
+        # every other bin: count / width / (float sum of all counts but the last)
+        norm = np.float32(0.0)
+        for v in c[:nb]:
+            norm = np.float32(float(norm) + v)
+        b = nb // 2
+        assert pdf[b] == counts[b - 1] / (edges[b] - edges[b - 1]) / float(norm)
+
+
+def test_spectrum_bin_log_x():
+    e = st.CPUHistogramUtils.BinLogX(60, -2.0, 4.0)
+    assert np.array_equal(e, po.bin_log_x(60, -2.0, 4.0))
+    assert abs(e[0] - 0.01) < 1e-15 and abs(e[-1] / 1e4 - 1) < 1e-14
+    assert np.all(np.diff(e) > 0)
+    rc = _capi.lib().st_spectrum_bin_log_x(0, 0.0, 1.0, None)
+    assert rc == _capi.ST_ERR_INVALID_ARGUMENT
