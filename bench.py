@@ -13,7 +13,8 @@ Metric: deposit*oversamples per second (higher is better).
   value : inputs resident in HBM, one batched run per step, device time (CUDA events on the
           stream the kernels run on), max over ranks;
   e2e   : the same through the public API with host (pinned) tracks: every step copies the
-          tracks host->device and reads every histogram back device->host.
+          tracks host->device (in groups on a second stream, overlapped with the kernels of
+          earlier groups) and reads every histogram back device->host.
 Multi-GPU (torchrun): every rank runs its own full workload (seed offset by rank), no
 collective on the data path (weak scaling); value = all ranks' units / max rank time.
 

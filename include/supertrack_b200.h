@@ -159,6 +159,10 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   shared_min_chunks  ... and exceed this many chunks                       (default 4)
  *   table_slots        shared-memory sphere table: 0 = 8192 slots when every histogram has at
  *                      most 700 bins, else 4096; 4096 = always 4096          (default 0)
+ *   pipeline_bytes     runs with host-resident tracks upload them in groups on a second stream
+ *                      while earlier groups compute; groups hold about this many bytes of
+ *                      track data (the first and last about a quarter); 0 = one upload, then
+ *                      one launch                                            (default 512 MiB)
  *   graphs             1 = a rerun of the same jobs replays a CUDA graph of the whole run
  *                      (captured at the first rerun); 0 = enqueue every call (default 1)
  *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to

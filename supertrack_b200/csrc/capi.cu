@@ -21,6 +21,7 @@ cudaError_t configure_fused();
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
+cudaError_t launch_reset_aux(JobAux* aux, int n, cudaStream_t s);
 }  // namespace st
 
 namespace {
@@ -163,6 +164,13 @@ struct st_ctx {
   const void* gexec_stage = nullptr;
   int64_t graph_launches = 0;
   int table_slots = 0;        // shared-memory sphere table: 0 automatic, 4096 or 8192
+  // pipelined runs of host tracks: jobs in groups of about pipeline_bytes of track data; the
+  // copy stream uploads group g+1 while the context's stream runs group g
+  int64_t pipeline_bytes = (int64_t)1 << 29;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> up_ev;
+  std::vector<int64_t> cache_blk;    // prepare-block prefix of the batch (host copy)
+  std::vector<char> cache_flagged;   // jobs with boundary flags
   float t_prep = 0, t_fused = 0;
   int32_t launches = 0;
 
@@ -174,7 +182,6 @@ struct st_ctx {
   // launch set-up of the last batched range, reused when the same jobs run again
   bool cache_valid = false;
   size_t cache_first = 0, cache_last = 0;
-  std::vector<JobAux> cache_aux;
   st::PrepareParams cache_pp{};
   st::FusedParams cache_fp{};
   int64_t cache_blocks = 0;
@@ -195,12 +202,11 @@ struct st_ctx {
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
   size_t h_aux_cap = 0;
-  PinnedBuf stage;                // job, histogram, prepare-block and aux tables of the run
+  PinnedBuf stage;                // job, histogram and prepare-block tables of the run
   // host time of the last launch (microseconds): whole launch, table building, allocations
   // inside it (and their number), the free-memory query
   double host_launch_us = 0, host_tables_us = 0, host_alloc_us = 0, host_meminfo_us = 0;
   int64_t host_allocs = 0;
-  size_t stage_aux_off = 0;
   int* h_err = nullptr;           // 4 ints + export count (8 bytes)
   bool pending = false;
   size_t pend_first = 0, pend_last = 0;
@@ -239,7 +245,8 @@ st_status init_spill_tables(st_ctx* c, uint32_t gcap, int grid) {
 
 // Copies the host-resident tracks of jobs [first, last) into the track arena; adjacent host
 // ranges are merged into one copy per coordinate array.
-st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena_total) {
+st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena_total,
+                             cudaStream_t stream) {
   double* arena = (double*)c->track_arena.p;
   size_t j = first;
   while (j < last) {
@@ -259,7 +266,7 @@ st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena
     const double* src[4] = {J.track.x, J.track.y, J.track.z, J.track.edep};
     for (int a = 0; a < 4; ++a)
       ST_CUDA(cudaMemcpyAsync(arena + (size_t)arena_total * a + J.arena_off, src[a],
-                              (size_t)n * 8, cudaMemcpyHostToDevice, c->stream),
+                              (size_t)n * 8, cudaMemcpyHostToDevice, stream),
               "track upload");
     j = k;
   }
@@ -294,7 +301,6 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   double* arena = (double*)c->track_arena.p;
 
   std::vector<JobDev> jd(nj);
-  std::vector<JobAux> aux(nj);
   std::vector<int64_t> blk(nj + 1, 0);
   int64_t cells_total = 0;
   bool any_flagged = false;
@@ -344,10 +350,6 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
       cells_total += D.cell_cap;
       any_flagged = true;
     }
-    JobAux& A = aux[i];
-    std::memset(&A, 0, sizeof(A));
-    A.e_min = 0x7fffffff;
-    A.e_max = (int32_t)0x80000000;
     blk[i + 1] = blk[i] + (J.n_pad + st::kPrepSlotsPerBlock - 1) / st::kPrepSlotsPerBlock;
   }
   std::vector<HistDev> hd(c->hists.size());
@@ -407,13 +409,11 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     // tables through pinned staging (the previous run's copies from it have completed)
     const size_t o_hists = align256(nj * sizeof(JobDev));
     const size_t o_blk = o_hists + align256(hd.size() * sizeof(HistDev));
-    const size_t o_aux = o_blk + align256((nj + 1) * 8);
-    ST_CUDA(ensure_pinned(c->stage, o_aux + align256(nj * sizeof(JobAux))), "pinned staging");
+    ST_CUDA(ensure_pinned(c->stage, o_blk + align256((nj + 1) * 8)), "pinned staging");
     char* st_base = (char*)c->stage.p;
     std::memcpy(st_base, jd.data(), nj * sizeof(JobDev));
     if (!hd.empty()) std::memcpy(st_base + o_hists, hd.data(), hd.size() * sizeof(HistDev));
     std::memcpy(st_base + o_blk, blk.data(), (nj + 1) * 8);
-    c->stage_aux_off = o_aux;
     ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, st_base, nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
     if (!hd.empty())
       ST_CUDA(cudaMemcpyAsync(c->d_hists.p, st_base + o_hists, hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
@@ -455,6 +455,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.jobs = (const JobDev*)c->d_jobs.p;
   pp.aux = (JobAux*)c->d_aux.p;
   pp.n_jobs = (int32_t)nj;
+  pp.blk_base = 0;
   pp.blk_prefix = (const int64_t*)c->d_blk.p;
   pp.blk_count = (int32_t*)c->d_blk_count.p;
   pp.blk_offset = (int64_t*)c->d_blk_off.p;
@@ -497,7 +498,9 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   fp.chunk_windows = c->chunk_windows;
   fp.pad2 = 0;
 
-  c->cache_aux = std::move(aux);
+  c->cache_blk = blk;
+  c->cache_flagged.resize(nj);
+  for (size_t i = 0; i < nj; ++i) c->cache_flagged[i] = (char)jd[i].flagged;
   c->cache_blocks = blk[nj];
   c->cache_grid = work_jobs == 0 ? 0 : grid;
   c->cache_item_cap = item_cap;
@@ -543,8 +546,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
 st_status enqueue_run(st_ctx* c, const st::FusedParams& fp, size_t nj, bool want_export,
                       bool capturing) {
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-  JobAux* st_aux = (JobAux*)((char*)c->stage.p + c->stage_aux_off);
-  ST_CUDA(cudaMemcpyAsync(c->d_aux.p, st_aux, nj * sizeof(JobAux), cudaMemcpyHostToDevice, c->stream), "upload aux");
+  ST_CUDA(st::launch_reset_aux((JobAux*)c->d_aux.p, (int)nj, c->stream), "reset aux");
   ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
   if (c->cache_grid > 0)
     ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
@@ -577,6 +579,65 @@ st_status enqueue_run(st_ctx* c, const st::FusedParams& fp, size_t nj, bool want
   ST_CUDA(cudaMemcpyAsync(c->h_err, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
   if (want_export) ST_CUDA(cudaMemcpyAsync(c->h_err + 4, c->ex_count.p, 8, cudaMemcpyDeviceToHost, c->stream), "read export count");
   ST_CUDA(cudaEventRecordWithFlags(c->ev[3], c->stream, evf), "event");
+  return ST_OK;
+}
+
+// Pipelined form of enqueue_run: after the batch-wide uploads and resets, each group of jobs
+// [groups[g], groups[g+1]) waits for its track upload, then runs its own prepare, plan and fused
+// launches on the jobs, aux and plan tables offset to its first job (the tables are batch-wide,
+// so every job keeps its slot). Events: 0 start, 1 and 4 before the first fused kernel, 2 after
+// the last one, 3 results copied.
+st_status enqueue_groups(st_ctx* c, const st::FusedParams& fp, size_t first,
+                         const std::vector<size_t>& groups) {
+  const size_t nj = groups.back() - first;
+  ST_CUDA(st::launch_reset_aux((JobAux*)c->d_aux.p, (int)nj, c->stream), "reset aux");
+  if (c->cache_cells > 0) {
+    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+  }
+  ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
+  ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
+  for (size_t g = 0; g + 1 < groups.size(); ++g) {
+    const size_t j0 = groups[g] - first, j1 = groups[g + 1] - first;
+    ST_CUDA(cudaStreamWaitEvent(c->stream, c->up_ev[g], 0), "upload wait");
+    ST_CUDA(cudaMemsetAsync(c->d_counter.p, 0, 16, c->stream), "reset counter");
+    if (c->cache_grid > 0)
+      ST_CUDA(cudaMemsetAsync(c->pool.p, 0, (size_t)((c->cache_grid + 31) / 32) * 4, c->stream), "pool reset");
+    ST_CUDA(cudaMemsetAsync(c->d_plan_misc.p, 0, 16 + 3 * 4 * st::kPlanBuckets, c->stream), "plan reset");
+    if (c->cache_units > 0) {
+      ST_CUDA(cudaMemsetAsync(c->u_next.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+      ST_CUDA(cudaMemsetAsync(c->u_done.p, 0, (size_t)c->cache_units * 4, c->stream), "unit reset");
+      ST_CUDA(cudaMemsetAsync(c->u_table.p, 0xFF, (size_t)c->cache_units * 4, c->stream), "unit reset");
+    }
+    st::PrepareParams pp = c->cache_pp;
+    pp.jobs += j0;
+    pp.aux += j0;
+    pp.n_jobs = (int32_t)(j1 - j0);
+    pp.blk_prefix += j0;
+    pp.blk_base = c->cache_blk[j0];
+    bool flagged = false;
+    for (size_t j = j0; j < j1; ++j) flagged |= c->cache_flagged[j] != 0;
+    ST_CUDA(st::launch_prepare(pp, c->cache_blk[j1] - c->cache_blk[j0], flagged, c->stream), "prepare launch");
+    st::PlanParams q = c->cache_plan;
+    q.jobs += j0;
+    q.aux += j0;
+    q.plan += j0;
+    q.n_jobs = (int32_t)(j1 - j0);
+    ST_CUDA(st::launch_plan(q, c->stream), "plan launch");
+    if (g == 0) {
+      ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+      ST_CUDA(cudaEventRecord(c->ev[4], c->stream), "event");
+    }
+    st::FusedParams f = fp;
+    f.jobs += j0;
+    f.aux += j0;
+    ST_CUDA(st::launch_fused(f, c->cache_max_nbins, c->cache_grid, c->table_slots, c->stream), "fused launch");
+  }
+  ST_CUDA(cudaEventRecord(c->ev[2], c->stream), "event");
+  ST_CUDA(cudaMemcpyAsync(c->h_aux, c->d_aux.p, nj * sizeof(JobAux), cudaMemcpyDeviceToHost, c->stream), "read aux");
+  ST_CUDA(cudaMemcpyAsync(c->h_err, c->d_err.p, 16, cudaMemcpyDeviceToHost, c->stream), "read errors");
+  ST_CUDA(cudaEventRecord(c->ev[3], c->stream), "event");
   return ST_OK;
 }
 
@@ -640,11 +701,54 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
     c->host_tables_us = now_us() - t_begin;
     if (s != ST_OK) { c->cache_valid = false; return s; }
   }
+  // groups of host track data (one group when every track is on the device): their uploads
+  // run on the copy stream, ahead of the groups' kernels. The first and the last group hold
+  // about a quarter of pipeline_bytes (the upload before the first kernels and the kernels after
+  // the last upload are not overlapped), the others about pipeline_bytes.
+  std::vector<size_t> groups(1, first);
   {
-    st_status s = upload_host_tracks(c, first, last, c->cache_arena_total);
-    if (s != ST_OK) return s;
+    int64_t total = 0;
+    for (size_t j = first; j < last; ++j)
+      if (!c->jobs[j].track.on_device) total += 32 * c->jobs[j].track.n;
+    const int64_t P = c->pipeline_bytes, q = std::max<int64_t>(P / 4, 1);
+    std::vector<int64_t> cuts;
+    if (total > 2 * q) {
+      for (int64_t t = q; t < total - q && cuts.size() < 62; t += P) cuts.push_back(t);
+      cuts.push_back(total - q);
+    }
+    int64_t acc = 0;
+    size_t k = 0;
+    for (size_t j = first; j < last && k < cuts.size(); ++j) {
+      if (!c->jobs[j].track.on_device) acc += 32 * c->jobs[j].track.n;
+      if (acc >= cuts[k] && j + 1 < last) {
+        groups.push_back(j + 1);
+        while (k < cuts.size() && acc >= cuts[k]) ++k;
+      }
+    }
+    groups.push_back(last);
   }
-  std::memcpy((char*)c->stage.p + c->stage_aux_off, c->cache_aux.data(), nj * sizeof(JobAux));
+  const bool pipelined = groups.size() > 2 && !want_export;
+  if (!pipelined) {
+    groups.assign({first, last});
+    st_status s = upload_host_tracks(c, first, last, c->cache_arena_total, c->stream);
+    if (s != ST_OK) return s;
+  } else {
+    if (!c->copy_stream)
+      ST_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+    while (c->up_ev.size() < groups.size()) {
+      cudaEvent_t e;
+      ST_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "upload event");
+      c->up_ev.push_back(e);
+    }
+    // the copies start after everything already queued on the context's stream
+    ST_CUDA(cudaEventRecord(c->up_ev.back(), c->stream), "event");
+    ST_CUDA(cudaStreamWaitEvent(c->copy_stream, c->up_ev.back(), 0), "copy stream wait");
+    for (size_t g = 0; g + 1 < groups.size(); ++g) {
+      st_status s = upload_host_tracks(c, groups[g], groups[g + 1], c->cache_arena_total, c->copy_stream);
+      if (s != ST_OK) return s;
+      ST_CUDA(cudaEventRecord(c->up_ev[g], c->copy_stream), "event");
+    }
+  }
 
   st::FusedParams fp = c->cache_fp;
   if (want_export) {
@@ -664,8 +768,13 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
   }
   if (!c->h_err) ST_CUDA(cudaMallocHost(&c->h_err, 32), "pinned flags");
 
-  const bool graph = reuse && c->use_graphs && !c->order_after;
+  const bool graph = reuse && c->use_graphs && !c->order_after && !pipelined;
   bool launched = false;
+  if (pipelined) {
+    st_status s = enqueue_groups(c, fp, first, groups);
+    if (s != ST_OK) return s;
+    launched = true;
+  }
   if (graph) {
     if (!c->gexec || c->gexec_build != c->build_id || c->gexec_aux != c->h_aux ||
         c->gexec_stage != c->stage.p)
@@ -680,8 +789,10 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
     st_status s = enqueue_run(c, fp, nj, want_export, false);
     if (s != ST_OK) return s;
   }
-  c->launches += (c->cache_blocks > 0 ? (c->cache_any_flagged ? 5 : 4) : 0) +
-                 (nj > 0 ? 4 : 0) + (c->cache_grid > 0 ? 1 : 0);
+  const size_t n_groups = groups.size() - 1;
+  c->launches += (nj > 0 ? 1 : 0) +
+                 (int32_t)n_groups * ((c->cache_blocks > 0 ? (c->cache_any_flagged ? 5 : 4) : 0) +
+                                      (nj > 0 ? 4 : 0) + (c->cache_grid > 0 ? 1 : 0));
   c->pending = true;
   c->pend_first = first;
   c->pend_last = last;
@@ -897,6 +1008,11 @@ st_status st_ctx_destroy(st_ctx* c) {
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};
   drop_graph(c);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
+  for (cudaEvent_t e : c->up_ev) cudaEventDestroy(e);
   for (DevBuf* b : bufs) release(*b);
   for (auto& e : c->ev) if (e) cudaEventDestroy(e);
   if (c->h_aux) cudaFreeHost(c->h_aux);
@@ -967,6 +1083,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
+  else if (n == "pipeline_bytes" && v >= 0) c->pipeline_bytes = v > 0 ? v : ((int64_t)1 << 62);
   else if (n == "graphs" && (v == 0 || v == 1)) { c->use_graphs = v != 0; drop_graph(c); }
   else return ST_ERR_INVALID_ARGUMENT;
   c->cache_valid = false;
@@ -984,6 +1101,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
+  else if (n == "pipeline_bytes") *v = c->pipeline_bytes;
   else if (n == "graphs") *v = c->use_graphs ? 1 : 0;
   else if (n == "graph_launches") *v = c->graph_launches;  // read-only: runs replayed from a graph
   else if (n == "last_grid") *v = c->cache_grid;       // read-only: CTAs of the last fused launch

@@ -253,6 +253,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   pp.ckeys = (uint64_t*)(base + L.ckeys);
   pp.cmin = (uint32_t*)(base + L.cmin);
   pp.cmax = (uint32_t*)(base + L.cmax);
+  pp.blk_base = 0;
   pp.PZ = (double*)(base + L.pz);
   pp.PX = (double*)(base + L.px);
   pp.PY = (double*)(base + L.py);

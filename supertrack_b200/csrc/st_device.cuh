@@ -143,6 +143,8 @@ struct PrepareParams {
   const JobDev* jobs;
   JobAux* aux;
   int32_t n_jobs;
+  int64_t blk_base;           // prepare block of blockIdx.x 0 (jobs and blk_prefix may start
+                              // at a later job of the batch; block indices stay batch-wide)
   const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
   int32_t* blk_count;         // kept deposits per prepare block
   int64_t* blk_offset;        // first kept index of each prepare block inside its job

@@ -115,7 +115,7 @@ __device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDe
 }
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
-  const int64_t b = blockIdx.x;
+  const int64_t b = p.blk_base + blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
   const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(1024) k_prep_scan(PrepareParams p) {
 }
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
-  const int64_t b = blockIdx.x;
+  const int64_t b = p.blk_base + blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
   const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
 // all non-boundary has no hit in any other window (its hits are within distance d of each other),
 // so the fused kernel can bin it as soon as the window is done.
 __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
-  const int64_t b = blockIdx.x;
+  const int64_t b = p.blk_base + blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
   if (!J.flagged) return;
@@ -1001,6 +1001,31 @@ __global__ void __launch_bounds__(128) k_plan_write(PlanParams q) {
     }
     q.items[pos] = w;
   }
+}
+
+// Job counters of a run to their initial values (exponent range empty, everything else zero).
+// A kernel rather than a copy from the host: a host-to-device copy on the run's stream would queue
+// on a copy engine behind any track upload in flight and hold the run's kernels back.
+__global__ void k_reset_aux(JobAux* aux, int n) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  JobAux a;
+  a.e_min = INT_MAX;
+  a.e_max = INT_MIN;
+  a.flags = 0;
+  a.pad = 0;
+  a.kept = 0;
+  a.hits = 0;
+  a.spheres = 0;
+  a.binned = 0;
+  a.inbox = 0;
+  aux[j] = a;
+}
+
+cudaError_t launch_reset_aux(JobAux* aux, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_reset_aux<<<(n + 255) / 256, 256, 0, s>>>(aux, n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s) {

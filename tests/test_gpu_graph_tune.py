@@ -92,3 +92,31 @@ def test_planning_parameters_do_not_change_results(work, name, value):
             c.run("batched")
             res.append(_spectra(c, hs))
     assert_hist_equal(res[1][0], res[1][1], res[0][0], res[0][1])
+
+
+def test_pipelined_host_tracks_equal_single_launch(work):
+    """Host tracks in several upload groups (copy stream ahead of each group's kernels) give the
+    same spectra and statistics as one upload and one launch."""
+    host = [t.cpu().numpy() for t in (work.x, work.y, work.z, work.edep)]
+    res = []
+    for pipeline_bytes in (0, 1 << 20):
+        with st.Context(0) as c:
+            c.set_param("pipeline_bytes", pipeline_bytes)
+            hs = [c.histogram(*h) for h in work.hists]
+            for j in range(work.n_jobs):
+                o, n = int(work.offsets[j]), int(work.sizes[j])
+                x, y, z, e = [a[o:o + n] for a in host]
+                c.submit(x, y, z, e, half_length=float(work.half_length[j]),
+                         sphere_diameter=float(work.diameter[j]),
+                         n_oversamples=int(work.n_os[j]), hist=hs[int(work.hist_of_job[j])],
+                         seed=int(work.seed[j]), track_id=int(work.track_id[j]),
+                         zshift=work.zshift)
+            for _ in range(2):                # the second run reuses the tables
+                c.jobs_reset()
+                c.run("batched")
+            res.append((_spectra(c, hs), [c.stats(j) for j in range(work.n_jobs)],
+                        c.last_timing()[2]))
+    ((c0, y0), s0, l0), ((c1, y1), s1, l1) = res
+    assert l1 > l0                            # the second form launched kernels per group
+    assert_hist_equal(c1, y1, c0, y0)
+    assert s0 == s1
