@@ -139,7 +139,7 @@ struct st_ctx {
   DevBuf track_arena;
   DevBuf px, py, pdz2, pvlo, pvhi, pkey;
   DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off;
-  DevBuf c_keys, c_min, c_max, pz;   // cell arena and shifted z of flagged jobs
+  DevBuf c_cells, pz;               // cell arena and shifted z of flagged jobs
   DevBuf u_next, u_done, u_table, pool;  // shared units and the spill-table pool
   DevBuf d_plan, d_plan_misc;             // planner: per-job plans and scratch counters
   DevBuf g_keys, g_lo, g_hi, g_used, g_count;
@@ -398,9 +398,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(ensure(c->d_hists, std::max<size_t>(1, hd.size()) * sizeof(HistDev)), "hist table");
   ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
   ST_CUDA(ensure(c->d_blk_count, (size_t)blk[nj] * 4), "prepare block counts");
-  ST_CUDA(ensure(c->c_keys, (size_t)cells_total * 8), "cell arena");
-  ST_CUDA(ensure(c->c_min, (size_t)cells_total * 4), "cell arena");
-  ST_CUDA(ensure(c->c_max, (size_t)cells_total * 4), "cell arena");
+  ST_CUDA(ensure(c->c_cells, (size_t)cells_total * sizeof(st::CellSlot)), "cell arena");
   ST_CUDA(ensure(c->pz, any_flagged ? (size_t)prep_total * 8 : 16), "shifted z");
   ST_CUDA(ensure(c->d_blk_off, (size_t)blk[nj] * 8), "prepare block offsets");
   ST_CUDA(ensure(c->d_counter, 16), "work counter");
@@ -459,9 +457,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.blk_prefix = (const int64_t*)c->d_blk.p;
   pp.blk_count = (int32_t*)c->d_blk_count.p;
   pp.blk_offset = (int64_t*)c->d_blk_off.p;
-  pp.ckeys = (uint64_t*)c->c_keys.p;
-  pp.cmin = (uint32_t*)c->c_min.p;
-  pp.cmax = (uint32_t*)c->c_max.p;
+  pp.cells = (st::CellSlot*)c->c_cells.p;
   pp.PZ = (double*)c->pz.p;
   pp.PX = (double*)c->px.p;
   pp.PY = (double*)c->py.p;
@@ -557,9 +553,7 @@ st_status enqueue_run(st_ctx* c, const st::FusedParams& fp, size_t nj, bool want
     ST_CUDA(cudaMemsetAsync(c->u_table.p, 0xFF, (size_t)c->cache_units * 4, c->stream), "unit reset");
   }
   if (c->cache_cells > 0) {
-    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_cells.p, 0xFF, (size_t)c->cache_cells * sizeof(st::CellSlot), c->stream), "cell reset");
   }
   ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
   if (want_export) ST_CUDA(cudaMemsetAsync(c->ex_count.p, 0, 16, c->stream), "export counter");
@@ -592,9 +586,7 @@ st_status enqueue_groups(st_ctx* c, const st::FusedParams& fp, size_t first,
   const size_t nj = groups.back() - first;
   ST_CUDA(st::launch_reset_aux((JobAux*)c->d_aux.p, (int)nj, c->stream), "reset aux");
   if (c->cache_cells > 0) {
-    ST_CUDA(cudaMemsetAsync(c->c_keys.p, 0xFF, (size_t)c->cache_cells * 8, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_min.p, 0xFF, (size_t)c->cache_cells * 4, c->stream), "cell reset");
-    ST_CUDA(cudaMemsetAsync(c->c_max.p, 0, (size_t)c->cache_cells * 4, c->stream), "cell reset");
+    ST_CUDA(cudaMemsetAsync(c->c_cells.p, 0xFF, (size_t)c->cache_cells * sizeof(st::CellSlot), c->stream), "cell reset");
   }
   ST_CUDA(cudaMemsetAsync(c->d_err.p, 0, 16, c->stream), "reset errors");
   ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
@@ -1002,8 +994,8 @@ st_status st_ctx_destroy(st_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pvlo, &c->pvhi, &c->pkey,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
-                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->c_keys,
-                    &c->c_min, &c->c_max, &c->pz, &c->u_next, &c->u_done, &c->u_table,
+                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->c_cells,
+                    &c->pz, &c->u_next, &c->u_done, &c->u_table,
                     &c->pool, &c->d_plan, &c->d_plan_misc, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,
                     &c->h_yfy, &c->h_edges};

@@ -50,7 +50,7 @@ constexpr size_t al(size_t v) { return (v + 255) / 256 * 256; }
 struct Layout {
   size_t jobs, aux, hists, blk_prefix, blk_count, blk_off;
   size_t px, py, pdz2, pvlo, pvhi, pkey, pz;
-  size_t ckeys, cmin, cmax;
+  size_t cells;
   size_t gkeys, glo, ghi, gused, gcount, pool;
   size_t items, plan, plan_misc, counter, err, edges, units;
   size_t total;
@@ -72,9 +72,7 @@ constexpr Layout make_layout() {
   L.pvhi = o;       o += al(kNaMaxDeposits * 8);
   L.pkey = o;       o += al(kNaMaxDeposits * 8);
   L.pz = o;         o += al(kNaMaxDeposits * 8);
-  L.ckeys = o;      o += al((size_t)kNaCellCap * 8);
-  L.cmin = o;       o += al((size_t)kNaCellCap * 4);
-  L.cmax = o;       o += al((size_t)kNaCellCap * 4);
+  L.cells = o;      o += al((size_t)kNaCellCap * sizeof(st::CellSlot));
   L.gkeys = o;      o += al((size_t)kNaGrid * kNaTableCap * 8);
   L.glo = o;        o += al((size_t)kNaGrid * kNaTableCap * 8);
   L.ghi = o;        o += al((size_t)kNaGrid * kNaTableCap * 8);
@@ -237,9 +235,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   NA_CUDA(cudaMemsetAsync(base + L.units, 0, 8, st_));
   NA_CUDA(cudaMemsetAsync(base + L.units + 8, 0xFF, 4, st_));
   if (D.flagged) {
-    NA_CUDA(cudaMemsetAsync(base + L.ckeys, 0xFF, (size_t)kNaCellCap * 8, st_));
-    NA_CUDA(cudaMemsetAsync(base + L.cmin, 0xFF, (size_t)kNaCellCap * 4, st_));
-    NA_CUDA(cudaMemsetAsync(base + L.cmax, 0, (size_t)kNaCellCap * 4, st_));
+    NA_CUDA(cudaMemsetAsync(base + L.cells, 0xFF, (size_t)kNaCellCap * sizeof(st::CellSlot), st_));
   }
 
   st::PrepareParams pp;
@@ -250,9 +246,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   pp.blk_prefix = (const int64_t*)(base + L.blk_prefix);
   pp.blk_count = (int32_t*)(base + L.blk_count);
   pp.blk_offset = (int64_t*)(base + L.blk_off);
-  pp.ckeys = (uint64_t*)(base + L.ckeys);
-  pp.cmin = (uint32_t*)(base + L.cmin);
-  pp.cmax = (uint32_t*)(base + L.cmax);
+  pp.cells = (st::CellSlot*)(base + L.cells);
   pp.blk_base = 0;
   pp.PZ = (double*)(base + L.pz);
   pp.PX = (double*)(base + L.px);

@@ -139,6 +139,16 @@ struct FusedParams {
   int32_t pad2;
 };
 
+// One slot of the cell hash used for boundary flags: the cell key (EMPTY when free), the
+// smallest window with a deposit in the cell and the bitwise complement of the largest one, so
+// that an all-ones fill is the empty state and both bounds are kept with atomicMin. One 16-byte
+// load reads a whole slot.
+struct __align__(16) CellSlot {
+  unsigned long long key;
+  unsigned int wmin;
+  unsigned int nwmax;
+};
+
 struct PrepareParams {
   const JobDev* jobs;
   JobAux* aux;
@@ -148,9 +158,7 @@ struct PrepareParams {
   const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
   int32_t* blk_count;         // kept deposits per prepare block
   int64_t* blk_offset;        // first kept index of each prepare block inside its job
-  uint64_t* ckeys;            // cell arena: cell key, EMPTY when free
-  uint32_t* cmin;             // smallest window with a deposit in the cell
-  uint32_t* cmax;             // largest window with a deposit in the cell
+  CellSlot* cells;            // cell arena (flagged jobs)
   double* PZ;                 // z after the z-origin shift (flagged jobs only)
   double* PX;
   double* PY;

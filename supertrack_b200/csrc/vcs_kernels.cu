@@ -84,16 +84,16 @@ __device__ __forceinline__ void cell_insert(const PrepareParams& p, const JobDev
   const uint32_t mask = J.cell_cap - 1;
   uint32_t h = slot_hash(key, mask);
   for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
-    uint64_t* slot = p.ckeys + J.cell_off + h;
-    const uint64_t k = __ldcg((const unsigned long long*)slot);
+    CellSlot* slot = p.cells + J.cell_off + h;
+    const uint64_t k = __ldcg(&slot->key);
     bool mine = k == key;
     if (!mine && k == kEmptyKey) {
-      const uint64_t old = atomicCAS((unsigned long long*)slot, kEmptyKey, key);
+      const uint64_t old = atomicCAS(&slot->key, kEmptyKey, key);
       mine = old == kEmptyKey || old == key;
     }
     if (mine) {
-      atomicMin(p.cmin + J.cell_off + h, win);
-      atomicMax(p.cmax + J.cell_off + h, win);
+      atomicMin(&slot->wmin, win);
+      atomicMin(&slot->nwmax, ~win);
       return;
     }
     h = (h + 1) & mask;
@@ -106,9 +106,9 @@ __device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDe
   const uint32_t mask = J.cell_cap - 1;
   uint32_t h = slot_hash(key, mask);
   for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
-    const uint64_t k = __ldcg((const unsigned long long*)(p.ckeys + J.cell_off + h));
-    if (k == key) return __ldcg(p.cmin + J.cell_off + h) != win || __ldcg(p.cmax + J.cell_off + h) != win;
-    if (k == kEmptyKey) return false;
+    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p.cells + J.cell_off + h));
+    if (v.x == key) return (uint32_t)v.y != win || ~(uint32_t)(v.y >> 32) != win;
+    if (v.x == kEmptyKey) return false;
     h = (h + 1) & mask;
   }
   return true;
@@ -374,8 +374,11 @@ template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
                                            const FusedParams& P, const Spill& G, uint64_t key,
                                            uint64_t lo, uint64_t hi, bool boundary) {
+  // A table of at least two windows' capacity is flushed at window ends once it is a quarter
+  // full (launch_fused), so it never passes three quarters and needs no per-insert check; a
+  // smaller one stops taking new spheres at three quarters (the rest go to the spill table).
   constexpr int kHardLimit = (CAP * 3) / 4;
-  if (*(volatile int*)&cs->tcount < kHardLimit) {
+  if (CAP >= 2 * kWindow || *(volatile int*)&cs->tcount < kHardLimit) {
     uint32_t h = slot_hash(key, CAP - 1);
 #pragma unroll 1
     for (int probe = 0; probe < 32; ++probe) {
@@ -1104,7 +1107,7 @@ cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots
   if (grid <= 0) return cudaSuccess;
   if (max_nbins <= kSmallHistBins && table_slots != 4096) {
     p.smem_hist_bins = kSmallHistBins;
-    p.flush_threshold = 8192 / 2;
+    p.flush_threshold = 8192 - 4096 - 8192 / 4;  // at most 3/4 full after the next window
     k_fused<8192, kFusedThreads>
         <<<grid, kFusedThreads, fused_smem_bytes(8192, kSmallHistBins), s>>>(p);
   } else {
