@@ -199,7 +199,7 @@ struct PlanParams {
 
 constexpr int kPrepThreads = 256;
 constexpr int kPrepSlotsPerBlock = 4 * kWarpTile;
-constexpr int kFusedWarps = 16;                       // warps of the fused kernel's CTA
+constexpr int kFusedWarps = 24;                       // warps of the fused kernel's CTA
 constexpr int kWindow = kFusedWarps * kWarpTile;      // kept deposits per window
 constexpr int kCellBits = 21;                         // bits per axis of a cell key
 

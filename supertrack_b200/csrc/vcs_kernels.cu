@@ -340,13 +340,30 @@ __device__ __forceinline__ bool gtable_add(uint64_t* gk, unsigned long long* glo
   return false;
 }
 
+// Dynamic shared memory of the fused kernel. The sphere table sits at fixed offsets (so that its
+// addresses cost no registers): keys, low and high accumulator words, the used-slot list and the
+// boundary bitmap; the shared-memory histogram (y*f(y), edges, counts) follows it.
+extern __shared__ __align__(16) unsigned char smem_raw[];
+
 template <int CAP>
 struct SmemTable {
-  uint64_t* keys;
-  unsigned long long* lo;
-  unsigned long long* hi;
-  uint16_t* used;
-  unsigned int* flags;   // CAP bits: the entry holds a boundary deposit's contribution
+  __device__ __forceinline__ static uint64_t* keys() { return reinterpret_cast<uint64_t*>(smem_raw); }
+  __device__ __forceinline__ static unsigned long long* lo() {
+    return reinterpret_cast<unsigned long long*>(smem_raw + 8 * CAP);
+  }
+  __device__ __forceinline__ static unsigned long long* hi() {
+    return reinterpret_cast<unsigned long long*>(smem_raw + 16 * CAP);
+  }
+  __device__ __forceinline__ static uint16_t* used() {
+    return reinterpret_cast<uint16_t*>(smem_raw + 24 * CAP);
+  }
+  // CAP bits: the entry holds a boundary deposit's contribution
+  __device__ __forceinline__ static unsigned int* flags() {
+    return reinterpret_cast<unsigned int*>(smem_raw + 26 * CAP);
+  }
+  __device__ __forceinline__ static double* hist() {
+    return reinterpret_cast<double*>(smem_raw + 26 * CAP + CAP / 8);
+  }
 };
 
 struct CtaState {
@@ -382,19 +399,19 @@ __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs
     uint32_t h = slot_hash(key, CAP - 1);
 #pragma unroll 1
     for (int probe = 0; probe < 32; ++probe) {
-      const uint64_t k = ((volatile uint64_t*)T.keys)[h];
+      const uint64_t k = ((volatile uint64_t*)T.keys())[h];
       bool mine = k == key;
       if (!mine && k == kEmptyKey) {
-        const uint64_t old = atomicCAS((unsigned long long*)&T.keys[h], kEmptyKey, key);
+        const uint64_t old = atomicCAS((unsigned long long*)&T.keys()[h], kEmptyKey, key);
         if (old == kEmptyKey) {
           const int idx = atomicAdd(&cs->tcount, 1);
-          T.used[idx] = (uint16_t)h;
+          T.used()[idx] = (uint16_t)h;
         }
         mine = old == kEmptyKey || old == key;
       }
       if (mine) {
-        acc_add(&T.lo[h], &T.hi[h], lo, hi);
-        if (boundary) atomicOr(&T.flags[h >> 5], 1u << (h & 31));
+        acc_add(&T.lo()[h], &T.hi()[h], lo, hi);
+        if (boundary) atomicOr(&T.flags()[h >> 5], 1u << (h & 31));
         return;
       }
       h = (h + 1) & (CAP - 1);
@@ -416,7 +433,6 @@ struct BinContext {
   int mode;               // 0: linear candidate, 1: log2 candidate
   double ca, cb;          // candidate bin = (y - ca) * cb, or (log2 y - ca) * cb
   int E0;
-  int os;
   int job;
 };
 
@@ -445,8 +461,7 @@ __device__ __forceinline__ int find_bin_fast(const BinContext& B, double y) {
 
 __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParams& P,
                                            uint64_t key, uint64_t lo, uint64_t hi,
-                                           unsigned long long& spheres,
-                                           unsigned long long& binned) {
+                                           unsigned int& spheres, unsigned int& binned, int os) {
   const double y = from_fixed(lo, hi, B.E0);
   ++spheres;
   const int b = find_bin_fast(B, y);
@@ -466,7 +481,7 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
       SphereRecord r;
       r.key = key;
       r.y = y;
-      r.os = B.os;
+      r.os = os;
       r.job = B.job;
       P.export_buf[idx] = r;
     } else {
@@ -480,12 +495,12 @@ template <int CAP, int THREADS>
 __device__ __forceinline__ void flush_to_spill(const SmemTable<CAP>& T, int cnt,
                                                const FusedParams& P, const Spill& G) {
   for (int i = threadIdx.x; i < cnt; i += THREADS) {
-    const uint32_t h = T.used[i];
-    if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
+    const uint32_t h = T.used()[i];
+    if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
       atomicOr(P.error_flags, 1);
-    T.keys[h] = kEmptyKey;
-    T.lo[h] = 0;
-    T.hi[h] = 0;
+    T.keys()[h] = kEmptyKey;
+    T.lo()[h] = 0;
+    T.hi()[h] = 0;
   }
 }
 
@@ -549,14 +564,14 @@ __device__ __forceinline__ Spill spill_of(const FusedParams& P, int t, long long
 // Bins and clears every entry of a spill table (all threads of the CTA).
 template <int THREADS>
 __device__ __forceinline__ void bin_spill(const Spill& G, const BinContext& B, const FusedParams& P,
-                                          unsigned long long& spheres, unsigned long long& binned) {
+                                          unsigned int& spheres, unsigned int& binned, int os) {
   const unsigned gc = __ldcg(G.count);
   for (unsigned i = threadIdx.x; i < gc; i += THREADS) {
     const uint32_t h = __ldcg(&G.used[i]);
     const uint64_t key = __ldcg((const unsigned long long*)&G.keys[h]);
     const uint64_t lo = __ldcg(&G.lo[h]);
     const uint64_t hi = __ldcg(&G.hi[h]);
-    bin_sphere(B, P, key, lo, hi, spheres, binned);
+    bin_sphere(B, P, key, lo, hi, spheres, binned, os);
     G.keys[h] = kEmptyKey; G.lo[h] = 0; G.hi[h] = 0;
   }
   __threadfence();
@@ -582,9 +597,8 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
                                             const SmemTable<CAP>& T, CtaState& cs,
                                             const Spill& G, const BinContext& B, int os,
                                             int64_t wt_begin, int64_t wt_end,
-                                            unsigned long long& hits, unsigned long long& inbox,
-                                            unsigned long long& spheres,
-                                            unsigned long long& binned) {
+                                            unsigned int& hits, unsigned int& inbox,
+                                            unsigned int& spheres, unsigned int& binned) {
   constexpr int kWarps = THREADS / 32;
   const JobDev& J = F.J;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -698,19 +712,19 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       const bool all_out = cs.overflow != 0;
       int sent = 0;
       for (int i = tid; i < cnt; i += THREADS) {
-        const uint32_t h = T.used[i];
-        const bool out = all_out || ((T.flags[h >> 5] >> (h & 31)) & 1u);
+        const uint32_t h = T.used()[i];
+        const bool out = all_out || ((T.flags()[h >> 5] >> (h & 31)) & 1u);
         if (out) {
-          if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys[h], T.lo[h], T.hi[h]))
+          if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
             atomicOr(P.error_flags, 1);
           sent = 1;
         } else {
-          bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
+          bin_sphere(B, P, T.keys()[h], T.lo()[h], T.hi()[h], spheres, binned, os);
         }
-        T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
+        T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
       }
       sent = __syncthreads_or(sent);
-      for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
+      for (int i = tid; i < CAP / 32; i += THREADS) T.flags()[i] = 0;
       if (tid == 0) {
         cs.tcount = 0;
         cs.overflow = 0;
@@ -739,27 +753,23 @@ template <int CAP, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   static_assert(CAP <= 65536, "used-slot list stores 16-bit slot indices");
   static_assert(THREADS / 32 == kFusedWarps, "a window is one CTA tile of warp tiles");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ CtaState cs;
   __shared__ int s_bcast[2];
+  __shared__ BinContext sB;   // the item's binning context and spill table, uniform over the
+  __shared__ Spill sG;        // CTA: kept in shared memory rather than in every thread's registers
 
   const int HB = P.smem_hist_bins;
-  SmemTable<CAP> T;
-  T.keys = reinterpret_cast<uint64_t*>(smem_raw);
-  T.lo = reinterpret_cast<unsigned long long*>(T.keys + CAP);
-  T.hi = T.lo + CAP;
-  double* hyfy = reinterpret_cast<double*>(T.hi + CAP);
+  const SmemTable<CAP> T;
+  double* hyfy = SmemTable<CAP>::hist();
   double* sedges = hyfy + HB;                                   // HB + 1 edges
   unsigned int* hcount = reinterpret_cast<unsigned int*>(sedges + HB + 1);
-  T.used = reinterpret_cast<uint16_t*>(hcount + HB);
-  T.flags = reinterpret_cast<unsigned int*>(T.used + CAP);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
 
-  for (int i = tid; i < CAP; i += THREADS) { T.keys[i] = kEmptyKey; T.lo[i] = 0; T.hi[i] = 0; }
+  for (int i = tid; i < CAP; i += THREADS) { T.keys()[i] = kEmptyKey; T.lo()[i] = 0; T.hi()[i] = 0; }
   for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
-  for (int i = tid; i < CAP / 32; i += THREADS) T.flags[i] = 0;
+  for (int i = tid; i < CAP / 32; i += THREADS) T.flags()[i] = 0;
   if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; cs.edges_hist = -1; }
   __syncthreads();
 
@@ -788,20 +798,24 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       if (tid == 0) cs.edges_hist = F.J.hist;
     }
 
-    BinContext B;
-    B.edges = smem_hist ? sedges : H.edges;
-    B.gcounts = H.counts;
-    B.gyfy = H.yfy;
-    B.nbins = H.nbins;
-    B.mode = H.mode;
-    B.ca = H.ca;
-    B.cb = H.cb;
-    B.E0 = F.E0;
-    B.job = W.job;
-    B.hcount = smem_hist ? hcount : nullptr;
-    B.hyfy = smem_hist ? hyfy : nullptr;
+    if (tid == 0) {
+      sB.edges = smem_hist ? sedges : H.edges;
+      sB.gcounts = H.counts;
+      sB.gyfy = H.yfy;
+      sB.nbins = H.nbins;
+      sB.mode = H.mode;
+      sB.ca = H.ca;
+      sB.cb = H.cb;
+      sB.E0 = F.E0;
+      sB.job = W.job;
+      sB.hcount = smem_hist ? hcount : nullptr;
+      sB.hyfy = smem_hist ? hyfy : nullptr;
+    }
+    __syncthreads();
+    const BinContext& B = sB;
 
-    unsigned long long hits = 0, spheres = 0, binned = 0, inbox = 0;
+    // per-thread counts of one item (an item covers at most a few million deposit*oversamples)
+    unsigned int hits = 0, spheres = 0, binned = 0, inbox = 0;
 
     // Segments: a private item walks its oversamples (all windows each) with one pool table; a
     // helper claims window chunks of its shared unit until none is left.
@@ -839,8 +853,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         wb = (int64_t)c * wpc;
         we = wb + wpc < F.n_wt ? wb + wpc : F.n_wt;
       }
-      B.os = os;
-      const Spill G = spill_of(P, t, A.kept);
+      if (tid == 0) sG = spill_of(P, t, A.kept);
+      __syncthreads();
+      const Spill& G = sG;
       superimpose<CAP, THREADS>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
       const int cnt = cs.tcount;
       bool bin_table;
@@ -850,9 +865,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
           flush_to_spill<CAP, THREADS>(T, cnt, P, G);
         } else {
           for (int i = tid; i < cnt; i += THREADS) {
-            const uint32_t h = T.used[i];
-            bin_sphere(B, P, T.keys[h], T.lo[h], T.hi[h], spheres, binned);
-            T.keys[h] = kEmptyKey; T.lo[h] = 0; T.hi[h] = 0;
+            const uint32_t h = T.used()[i];
+            bin_sphere(B, P, T.keys()[h], T.lo()[h], T.hi()[h], spheres, binned, os);
+            T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
           }
         }
         __syncthreads();
@@ -870,7 +885,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         if (bin_table) __threadfence();
       }
       if (bin_table) {
-        bin_spill<THREADS>(G, B, P, spheres, binned);
+        bin_spill<THREADS>(G, B, P, spheres, binned, os);
         if (shared && tid == 0) pool_release(P.pool_bits, t);
       }
       if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; }
@@ -894,18 +909,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         }
       }
     }
+    unsigned long long w_hits = hits, w_spheres = spheres, w_binned = binned, w_inbox = inbox;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      hits += __shfl_xor_sync(0xffffffffu, hits, o);
-      spheres += __shfl_xor_sync(0xffffffffu, spheres, o);
-      binned += __shfl_xor_sync(0xffffffffu, binned, o);
-      inbox += __shfl_xor_sync(0xffffffffu, inbox, o);
+      w_hits += __shfl_xor_sync(0xffffffffu, w_hits, o);
+      w_spheres += __shfl_xor_sync(0xffffffffu, w_spheres, o);
+      w_binned += __shfl_xor_sync(0xffffffffu, w_binned, o);
+      w_inbox += __shfl_xor_sync(0xffffffffu, w_inbox, o);
     }
     if (lane == 0) {
-      if (hits) atomicAdd(&P.aux[W.job].hits, hits);
-      if (spheres) atomicAdd(&P.aux[W.job].spheres, spheres);
-      if (binned) atomicAdd(&P.aux[W.job].binned, binned);
-      if (inbox) atomicAdd(&P.aux[W.job].inbox, inbox);
+      if (w_hits) atomicAdd(&P.aux[W.job].hits, w_hits);
+      if (w_spheres) atomicAdd(&P.aux[W.job].spheres, w_spheres);
+      if (w_binned) atomicAdd(&P.aux[W.job].binned, w_binned);
+      if (w_inbox) atomicAdd(&P.aux[W.job].inbox, w_inbox);
     }
     __syncthreads();
   }
@@ -1067,7 +1083,7 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s
 // ---------------------------------------------------------------------------------------------
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------------------------
-constexpr int kFusedThreads = 512;
+constexpr int kFusedThreads = 768;
 
 // Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
 // 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
