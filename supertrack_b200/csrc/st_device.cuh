@@ -20,7 +20,7 @@
 
 namespace st {
 
-constexpr int kDepPerLane = 8;                  // deposits owned by one lane inside a warp tile
+constexpr int kDepPerLane = 4;                  // deposits owned by one lane inside a warp tile
 constexpr int kWarpTile = 32 * kDepPerLane;     // deposits per warp tile
 constexpr uint64_t kEmptyKey = ~0ull;           // never a valid sphere key (keys < 2^63)
 
@@ -198,8 +198,8 @@ struct PlanParams {
 };
 
 constexpr int kPrepThreads = 256;
-constexpr int kPrepSlotsPerBlock = 4 * kWarpTile;
-constexpr int kFusedWarps = 24;                       // warps of the fused kernel's CTA
+constexpr int kPrepSlotsPerBlock = 1024;                // source deposits per prepare block
+constexpr int kFusedWarps = 32;                       // warps of the fused kernel's CTA
 constexpr int kWindow = kFusedWarps * kWarpTile;      // kept deposits per window
 constexpr int kCellBits = 21;                         // bits per axis of a cell key
 

@@ -33,6 +33,7 @@ __device__ __forceinline__ uint32_t slot_hash(uint64_t key, uint32_t mask) {
 // ---------------------------------------------------------------------------------------------
 constexpr double kMagic = 0x1.8p52;             // adding it rounds |q| < 2^51 to an integer
 constexpr double kRiskBand = 0.5 - 0x1p-20;     // |q - rint(q)| at or above it: decide exactly
+constexpr int kGeoBlock = 2;                     // deposits per straight-line geometry block
 
 // ---------------------------------------------------------------------------------------------
 // Prepare stage (once per track): four launches.
@@ -613,13 +614,13 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       const int64_t tb = J.prep_off + w * kWarpTile + lane;
       uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
       unsigned hitmask = 0, boxmask = 0;
-      // geometry in straight-line blocks of four deposits, so their FP64 chains interleave
+      // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
 #pragma unroll
-      for (int h4 = 0; h4 < kDepPerLane; h4 += 4) {
-        double ax[4], ay[4], kdx[4], kdy[4];
+      for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
+        double ax[kGeoBlock], ay[kGeoBlock], kdx[kGeoBlock], kdy[kGeoBlock];
         unsigned risk = 0;
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
+        for (int p = 0; p < kGeoBlock; ++p) {
           const double x1 = st_dadd(__ldg(&P.PX[tb + (h4 + p) * 32]), sx);
           const double y1 = st_dadd(__ldg(&P.PY[tb + (h4 + p) * 32]), sy);
           const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
@@ -639,7 +640,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
           // quotients (|q| < 2^21); only a quotient this close to a half-integer can round
           // differently, and then the IEEE division decides (rare: lattice-aligned inputs)
 #pragma unroll
-          for (int p = 0; p < 4; ++p) {
+          for (int p = 0; p < kGeoBlock; ++p) {
             if (risk & (1u << p)) {
               kdx[p] = rint(__ddiv_rn(ax[p], J.d));
               kdy[p] = rint(__ddiv_rn(ay[p], J.d));
@@ -647,7 +648,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
           }
         }
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
+        for (int p = 0; p < kGeoBlock; ++p) {
           const double ddx = st_dsub(st_dmul(kdx[p], J.d), ax[p]);
           const double ddy = st_dsub(st_dmul(kdy[p], J.d), ay[p]);
           const double dz2 = __ldg(&P.PDZ2[tb + (h4 + p) * 32]);
@@ -1083,7 +1084,9 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s
 // ---------------------------------------------------------------------------------------------
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------------------------
-constexpr int kFusedThreads = 768;
+// 32 warps (64 registers each): the kernel is latency-bound, and more resident warps hide more
+// of it than longer per-thread blocks would.
+constexpr int kFusedThreads = 1024;
 
 // Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
 // 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
