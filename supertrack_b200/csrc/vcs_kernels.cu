@@ -367,11 +367,15 @@ struct SmemTable {
   }
 };
 
+// Occupancy and overflow of the sphere table are counted per window in one of three rotating
+// slots (window i uses slot i % 3; a job without window flags always uses slot 0): the slot of the
+// next window can then be cleared while the current window's is still being read, which saves a
+// CTA barrier per window.
 struct CtaState {
   int item;
-  int tcount;
+  int tc[3];        // used slots of the table (the used-list length) in this window
   int spilled;      // some sphere of this oversample has a partial sum in the spill table
-  int overflow;     // this window sent a contribution to the spill table directly
+  int ovf[3];       // this window sent a contribution to the spill table directly
   int edges_hist;   // histogram whose edges are in shared memory (-1: none)
 };
 
@@ -391,12 +395,12 @@ struct Spill {
 template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
                                            const FusedParams& P, const Spill& G, uint64_t key,
-                                           uint64_t lo, uint64_t hi, bool boundary) {
+                                           uint64_t lo, uint64_t hi, bool boundary, int slot) {
   // A table of at least two windows' capacity is flushed at window ends once it is a quarter
   // full (launch_fused), so it never passes three quarters and needs no per-insert check; a
   // smaller one stops taking new spheres at three quarters (the rest go to the spill table).
   constexpr int kHardLimit = (CAP * 3) / 4;
-  if (CAP >= 2 * kWindow || *(volatile int*)&cs->tcount < kHardLimit) {
+  if (CAP >= 2 * kWindow || *(volatile int*)&cs->tc[slot] < kHardLimit) {
     uint32_t h = slot_hash(key, CAP - 1);
 #pragma unroll 1
     for (int probe = 0; probe < 32; ++probe) {
@@ -405,7 +409,7 @@ __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs
       if (!mine && k == kEmptyKey) {
         const uint64_t old = atomicCAS((unsigned long long*)&T.keys()[h], kEmptyKey, key);
         if (old == kEmptyKey) {
-          const int idx = atomicAdd(&cs->tcount, 1);
+          const int idx = atomicAdd(&cs->tc[slot], 1);
           T.used()[idx] = (uint16_t)h;
         }
         mine = old == kEmptyKey || old == key;
@@ -419,7 +423,7 @@ __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs
     }
   }
   *(volatile int*)&cs->spilled = 1;
-  *(volatile int*)&cs->overflow = 1;
+  *(volatile int*)&cs->ovf[slot] = 1;
   if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, key, lo, hi))
     atomicOr(P.error_flags, 1);
 }
@@ -608,7 +612,13 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   const double sx = shift_from_uniform(ux, J.L, J.HL);
   const double sy = shift_from_uniform(uy, J.L, J.HL);
 
+  // a job without window flags whose whole lattice (N^3 spheres) stays below the flush
+  // threshold can never need a flush between windows: its windows run without a barrier
+  const bool window_checks =
+      !J.flagged && (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
+  int wi = 0;  // window index within this call
   for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps) {
+    const int slot = J.flagged ? wi % 3 : 0;
     const int64_t w = wt0 + warp;
     if (w < wt_end) {
       const int64_t tb = J.prep_off + w * kWarpTile + lane;
@@ -677,7 +687,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
             add128(rlo, rhi, lo, hi);
             rflag |= bflag;
           } else {
-            if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
+            if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
             rkey = key; rlo = lo; rhi = hi; rflag = bflag;
           }
         }
@@ -702,19 +712,26 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
             head = ohead;
           }
         }
-        if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag);
+        if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
       }
     }
     if (J.flagged) {
       // window done: spheres without boundary contributions are complete -> bin them now;
       // the others (or all, if the window overflowed) go to the spill table
       __syncthreads();
-      const int cnt = cs.tcount;
-      const bool all_out = cs.overflow != 0;
+      const int cnt = cs.tc[slot];
+      const bool all_out = cs.ovf[slot] != 0;
+      if (tid == 0) {  // the next window's slot: last read two windows ago
+        cs.tc[(wi + 1) % 3] = 0;
+        cs.ovf[(wi + 1) % 3] = 0;
+      }
       int sent = 0;
       for (int i = tid; i < cnt; i += THREADS) {
         const uint32_t h = T.used()[i];
-        const bool out = all_out || ((T.flags()[h >> 5] >> (h & 31)) & 1u);
+        const unsigned bit = 1u << (h & 31);
+        const bool flagged = (T.flags()[h >> 5] & bit) != 0;
+        if (flagged) atomicAnd(&T.flags()[h >> 5], ~bit);
+        const bool out = all_out || flagged;
         if (out) {
           if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
             atomicOr(P.error_flags, 1);
@@ -724,23 +741,19 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         }
         T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
       }
+      // the table and its boundary bits are clear again once every thread is past this point
       sent = __syncthreads_or(sent);
-      for (int i = tid; i < CAP / 32; i += THREADS) T.flags()[i] = 0;
-      if (tid == 0) {
-        cs.tcount = 0;
-        cs.overflow = 0;
-        if (sent) cs.spilled = 1;
-      }
+      if (sent && tid == 0) cs.spilled = 1;
+    } else if (window_checks && wt0 + kWarps < wt_end) {
       __syncthreads();
-    } else if (wt0 + kWarps < wt_end) {
-      __syncthreads();
-      if (cs.tcount > P.flush_threshold) {
-        flush_to_spill<CAP, THREADS>(T, cs.tcount, P, G);
+      if (cs.tc[0] > P.flush_threshold) {
+        flush_to_spill<CAP, THREADS>(T, cs.tc[0], P, G);
         __syncthreads();
-        if (tid == 0) { cs.tcount = 0; cs.spilled = 1; }
+        if (tid == 0) { cs.tc[0] = 0; cs.spilled = 1; }
         __syncthreads();
       }
     }
+    ++wi;
   }
   __syncthreads();
 }
@@ -771,7 +784,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   for (int i = tid; i < CAP; i += THREADS) { T.keys()[i] = kEmptyKey; T.lo()[i] = 0; T.hi()[i] = 0; }
   for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
   for (int i = tid; i < CAP / 32; i += THREADS) T.flags()[i] = 0;
-  if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; cs.edges_hist = -1; }
+  if (tid == 0) {
+    for (int k = 0; k < 3; ++k) { cs.tc[k] = 0; cs.ovf[k] = 0; }
+    cs.spilled = 0;
+    cs.edges_hist = -1;
+  }
   __syncthreads();
 
   for (;;) {
@@ -858,7 +875,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       __syncthreads();
       const Spill& G = sG;
       superimpose<CAP, THREADS>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
-      const int cnt = cs.tcount;
+      const int cnt = F.J.flagged ? 0 : cs.tc[0];  // flagged windows leave the table empty
       bool bin_table;
       if (!shared) {
         bin_table = cs.spilled != 0;
@@ -889,7 +906,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         bin_spill<THREADS>(G, B, P, spheres, binned, os);
         if (shared && tid == 0) pool_release(P.pool_bits, t);
       }
-      if (tid == 0) { cs.tcount = 0; cs.spilled = 0; cs.overflow = 0; }
+      if (tid == 0) {
+        for (int k = 0; k < 3; ++k) { cs.tc[k] = 0; cs.ovf[k] = 0; }
+        cs.spilled = 0;
+      }
       __syncthreads();
     }
     if (private_table >= 0) {
