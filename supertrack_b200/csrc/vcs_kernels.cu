@@ -428,12 +428,15 @@ __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs
     atomicOr(P.error_flags, 1);
 }
 
+constexpr int kHistCopies = 4;   // at most this many shared-memory copies of a histogram
+
 struct BinContext {
   const double* edges;    // shared-memory copy when the histogram fits, else HBM
   unsigned long long* gcounts;
   double* gyfy;
   unsigned int* hcount;   // null: accumulate straight into HBM
   double* hyfy;
+  int copies;             // shared-memory copies of the histogram, used by warp % copies
   int nbins;
   int mode;               // 0: linear candidate, 1: log2 candidate
   double ca, cb;          // candidate bin = (y - ca) * cb, or (log2 y - ca) * cb
@@ -473,8 +476,10 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
   if (b >= 0) {
     ++binned;
     if (B.hcount) {
-      atomicAdd(&B.hcount[b], 1u);
-      atomicAdd(&B.hyfy[b], y);
+      // warps spread over the copies, so that fewer of them contend for a bin's 64-bit add
+      const int c = B.copies > 1 ? (int)((threadIdx.x >> 5) % (unsigned)B.copies) * B.nbins : 0;
+      atomicAdd(&B.hcount[c + b], 1u);
+      atomicAdd(&B.hyfy[c + b], y);
     } else {
       atomicAdd(&B.gcounts[b], 1ull);
       atomicAdd(&B.gyfy[b], y);
@@ -828,6 +833,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       sB.job = W.job;
       sB.hcount = smem_hist ? hcount : nullptr;
       sB.hyfy = smem_hist ? hyfy : nullptr;
+      sB.copies = smem_hist ? min(kHistCopies, HB / H.nbins) : 1;
     }
     __syncthreads();
     const BinContext& B = sB;
@@ -920,13 +926,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
 
     // ---- per-item flush of the shared-memory histogram and the job statistics
     if (smem_hist) {
+      const int copies = B.copies;
       for (int b = tid; b < H.nbins; b += THREADS) {
-        const unsigned cnt = hcount[b];
+        unsigned cnt = 0;
+        double ys = 0.0;
+        for (int c = 0; c < copies; ++c) {
+          const int i = c * H.nbins + b;
+          cnt += hcount[i];
+          ys += hyfy[i];
+          hcount[i] = 0;
+          hyfy[i] = 0.0;
+        }
         if (cnt) {
           atomicAdd(&H.counts[b], (unsigned long long)cnt);
-          atomicAdd(&H.yfy[b], hyfy[b]);
-          hcount[b] = 0;
-          hyfy[b] = 0.0;
+          atomicAdd(&H.yfy[b], ys);
         }
       }
     }
