@@ -1124,7 +1124,7 @@ constexpr int kFusedThreads = 1024;
 // Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
 // 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
 // most kSmallHistBins bins.
-constexpr int kSmallHistBins = 700;
+constexpr int kSmallHistBins = 900;
 constexpr int kBigHistBins = 4096;
 
 size_t fused_smem_bytes(int cap, int hist_bins) {
