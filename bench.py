@@ -64,6 +64,8 @@ def parse():
                    help="track-count scale of the workload (1.0 = as specified)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-fp32", action="store_true",
+                   help="skip the FP32 geometry variant's leg (reported beside the FP64 value)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-tune", action="store_true",
                    help="skip the autotuner (default planning parameters)")
@@ -394,6 +396,59 @@ def ours(args, rank, world):
         plain = {"value": pval, "unit": UNIT, "batched_over_plain": value / pval,
                  "timing": "host wall clock around the per-track loop (one sync per track)"}
 
+    # ---- FP32 geometry variant on the same jobs (not the headline: it is not bound to the
+    # reference's FP64 results); its spectra are compared with one FP64 run of the same jobs
+    fp32 = None
+    if not args.no_fp32:
+        nb = ctx.total_bins()
+        spectra = {}
+        for prec in (64, 32):
+            ctx.set_param("precision", prec)
+            ctx.clear_histograms()
+            ctx.jobs_reset()
+            ctx.run("batched")
+            c_ = torch.empty(nb, dtype=torch.int64)
+            y_ = torch.empty(nb, dtype=torch.float64)
+            ctx.read_all_into(c_.data_ptr(), y_.data_ptr(), nb)
+            st_ = [ctx.stats(j) for j in range(w.n_jobs)]
+            spectra[prec] = (c_.numpy().copy(), sum(s["hits"] for s in st_),
+                             sum(s["spheres"] for s in st_), sum(s["binned"] for s in st_))
+        for _ in range(args.warmup):
+            ctx.jobs_reset()
+            ctx.run("batched")
+        barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        f_prep = f_fused = 0.0
+        for _ in range(args.steps):
+            ctx.jobs_reset()
+            ctx.run("batched")
+            a, b, _n = ctx.last_timing()
+            f_prep += a
+            f_fused += b
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        fms = torch.tensor([f0.elapsed_time(f1)], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(fms, op=torch.distributed.ReduceOp.MAX)
+        ctx.set_param("precision", 64)
+        c64, h64, s64, b64 = spectra[64]
+        c32, h32, s32, b32 = spectra[32]
+        fp32 = {"value": units * world * args.steps / (float(fms.item()) * 1e-3), "unit": UNIT,
+                "ms_per_step": float(fms.item()) / args.steps,
+                "kernel_ms": {"prepare": f_prep / args.steps, "fused": f_fused / args.steps},
+                "fp64_run": {"hits": h64, "spheres": s64, "binned": b64},
+                "diff_vs_fp64": {"hits": h32 - h64, "spheres": s32 - s64, "binned": b32 - b64,
+                                 "counts_l1": int(np.abs(c32 - c64).sum())},
+                "hits_rel_diff": (h32 - h64) / max(h64, 1),
+                "spheres_rel_diff": (s32 - s64) / max(s64, 1),
+                "counts_l1_rel": float(np.abs(c32 - c64).sum()) / max(float(c64.sum()), 1.0),
+                "note": "FP32 geometry variant (x/y geometry in float; z, keys and energies as "
+                        "FP64): reported beside the FP64 value, not bound to reference parity"}
+
     if rank != 0:
         ctx.close()
         return
@@ -446,6 +501,7 @@ def ours(args, rank, world):
         "clocks": clocks,
         "e2e": e2e,
         "plain": plain,
+        "fp32": fp32,
         "cpu_baseline": cpu,
         "serving": None,
     }

@@ -157,6 +157,11 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   share_divisor      a job runs as shared units (one per oversample) when its kept deposits
  *                      exceed batch units / (share_divisor * grid); 0 = never (default 8)
  *   shared_min_chunks  ... and exceed this many chunks                       (default 4)
+ *   precision          64 = the reference's FP64 arithmetic; 32 = FP32 geometry variant: x, y,
+ *                      shifts, the x/y box test, x/y lattice index and sphere distance in float
+ *                      (z, keys and energies as in FP64). No reference counterpart: the
+ *                      reference's readme asks for a float form (readme.md:29). Results are
+ *                      not bound to the reference's                           (default 64)
  *   table_slots        shared-memory sphere table: 0 = 8192 slots when every histogram has at
  *                      most 900 bins, else 4096; 4096 = always 4096          (default 0)
  *   pipeline_bytes     runs with host-resident tracks upload them in groups on a second stream

@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
                                                 C.POINTER(or_stats), C.c_void_p, C.c_int64,
                                                 C.POINTER(C.c_int64)]
         h.or_job.restype = C.c_int
+        h.or_job_f32.argtypes = h.or_job.argtypes
+        h.or_job_f32.restype = C.c_int
         h.or_run_batch.argtypes = [C.c_int64] + [C.c_void_p] * 20 + [C.c_int32]
         h.or_run_batch.restype = C.c_int
         _lib = h
@@ -113,8 +115,9 @@ ZS = {"plus": 0, "minus": 1, "none": 2}
 
 
 def run_job(x, y, z, edep, *, half_length, sphere_diameter, sxsy, edges_arr, zshift="plus",
-            sum_mode=OR_SUM_EXACT, spheres_cap=0, counts=None, yfy=None):
-    """One job through the oracle; returns (counts, yfy, stats dict, spheres array or None)."""
+            sum_mode=OR_SUM_EXACT, spheres_cap=0, counts=None, yfy=None, precision=64):
+    """One job through the oracle; returns (counts, yfy, stats dict, spheres array or None).
+    precision 32 runs the FP32 geometry variant (or_job_f32)."""
     arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, edep)]
     n = len(arrs[0])
     sx = np.ascontiguousarray(sxsy, dtype=np.float64).reshape(-1)
@@ -128,7 +131,8 @@ def run_job(x, y, z, edep, *, half_length, sphere_diameter, sxsy, edges_arr, zsh
     st = or_stats()
     sph = np.zeros(max(spheres_cap, 1), dtype=SPHERE_DTYPE) if spheres_cap else None
     nsph = C.c_int64(0)
-    rc = lib().or_job(*[_p(a) for a in arrs], n, half_length, sphere_diameter, ZS[zshift],
+    fn = lib().or_job_f32 if precision == 32 else lib().or_job
+    rc = fn(*[_p(a) for a in arrs], n, half_length, sphere_diameter, ZS[zshift],
                       n_os, _p(sx) if n_os else None, _p(e), nb, sum_mode, _p(counts), _p(yfy),
                       C.byref(st), _p(sph) if sph is not None else None, spheres_cap,
                       C.byref(nsph))

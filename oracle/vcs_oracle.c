@@ -21,6 +21,7 @@
  *   key and value       VoxelConstrainedSphereMethod.cu:302-322
  *   reduce + binning    Histogram.cu:150-158 (sort by key, sum per key, HistogramRange [lo,hi))
  *   accumulation        Histogram.cu:161-171, SuperTrackManager.cu:71-75 (per oversample, summed)
+ *   FP32 variant        or_job_f32: the readme's float wish (readme.md:29), no reference code
  *
  * Per-sphere sums: the reference's CUB sort + ReduceByKey order is not deterministic, so the
  * oracle fixes two definitions:
@@ -238,10 +239,11 @@ static int bin_of(const double* e, int nbins, double y) {
  * the number produced even when it exceeds cap). Returns 0, or 1 bad geometry, 2 non-finite
  * contribution, 3 out of memory.
  */
-int or_job(const double* x, const double* y, const double* z, const double* edep, int64_t n,
-           double half_length, double d, int zshift_mode, uint32_t n_os, const double* sxsy,
-           const double* edges, int nbins, int sum_mode, int64_t* counts, double* yfy,
-           or_stats* st, or_sphere* spheres_out, int64_t cap, int64_t* n_spheres) {
+static int job_impl(const double* x, const double* y, const double* z, const double* edep,
+                    int64_t n, double half_length, double d, int zshift_mode, uint32_t n_os,
+                    const double* sxsy, const double* edges, int nbins, int sum_mode,
+                    int64_t* counts, double* yfy, or_stats* st, or_sphere* spheres_out,
+                    int64_t cap, int64_t* n_spheres, int fp32) {
   or_geom g;
   if (or_geometry(half_length, d, &g)) return 1;
   const double zsh = zshift_mode == 0 ? g.HL : (zshift_mode == 1 ? -g.HL : 0.0);
@@ -278,23 +280,53 @@ int or_job(const double* x, const double* y, const double* z, const double* edep
 
   for (uint32_t os = 0; os < n_os; os++) {
     const double sx = sxsy[2 * os], sy = sxsy[2 * os + 1];
-    /* FilterInScoringBox */
+    /* FilterInScoringBox (FP32 form: x, y and the shift rounded to float, the sum in float;
+       the float results are held exactly in bx/by) */
+    const float f_sx = (float)sx, f_sy = (float)sy, f_HL = (float)g.HL;
     int64_t nbox = 0;
     for (int64_t i = 0; i < n; i++) {
-      double xs = x[i] + sx, ys = y[i] + sy;
-      if (fabs(xs) < g.HL && fabs(ys) < g.HL && fabs(zs[i]) < g.HL) {
+      double xs, ys;
+      int in;
+      if (fp32) {
+        const float fx = (float)x[i] + f_sx, fy = (float)y[i] + f_sy;
+        xs = fx; ys = fy;
+        in = fabsf(fx) < f_HL && fabsf(fy) < f_HL;
+      } else {
+        xs = x[i] + sx; ys = y[i] + sy;
+        in = fabs(xs) < g.HL && fabs(ys) < g.HL;
+      }
+      if (in && fabs(zs[i]) < g.HL) {
         bx[nbox] = xs; by[nbox] = ys; bi[nbox] = i; nbox++;
       }
     }
-    /* FilterTrackInSphere + ScoreTrackInSphere */
+    /* FilterTrackInSphere + ScoreTrackInSphere (FP32 form: a = x' - gSO, k = rint(a * (1/d)),
+       dx = k*d - a and dist = (dx^2 + dy^2) + RN32(dz^2) in float; z as in the FP64 form) */
+    const float f_gSO = (float)g.gSO, f_d = (float)g.d, f_inv_d = 1.0f / f_d;
+    const float f_r2 = (float)r2;
     int64_t nh = 0;
     for (int64_t k = 0; k < nbox; k++) {
       const int64_t i = bi[k];
-      double ax = bx[k] - g.gSO, ay = by[k] - g.gSO, az = zs[i] - g.gSO;
-      long long kx = llrint(ax / g.d), ky = llrint(ay / g.d), kz = llrint(az / g.d);
-      double dx = (kx * g.d) - ax, dy = (ky * g.d) - ay, dz = (kz * g.d) - az;
-      double dist = (dx * dx) + (dy * dy) + (dz * dz);
-      if (dist <= r2) {
+      long long kx, ky, kz;
+      int hit;
+      if (fp32) {
+        const float ax = (float)bx[k] - f_gSO, ay = (float)by[k] - f_gSO;
+        const float fkx = rintf(ax * f_inv_d), fky = rintf(ay * f_inv_d);
+        const float dx = (fkx * f_d) - ax, dy = (fky * f_d) - ay;
+        const double az = zs[i] - g.gSO;
+        kz = llrint(az / g.d);
+        const double dz = (kz * g.d) - az;
+        const float dist = ((dx * dx) + (dy * dy)) + (float)(dz * dz);
+        kx = (long long)fkx;
+        ky = (long long)fky;
+        hit = dist <= f_r2;
+      } else {
+        double ax = bx[k] - g.gSO, ay = by[k] - g.gSO, az = zs[i] - g.gSO;
+        kx = llrint(ax / g.d); ky = llrint(ay / g.d); kz = llrint(az / g.d);
+        double dx = (kx * g.d) - ax, dy = (ky * g.d) - ay, dz = (kz * g.d) - az;
+        double dist = (dx * dx) + (dy * dy) + (dz * dz);
+        hit = dist <= r2;
+      }
+      if (hit) {
         hits[nh].key = (uint64_t)kx + (uint64_t)ky * N + (uint64_t)kz * N * N;
         hits[nh].idx = i;
         hits[nh].v = edep[i] / lineal;
@@ -338,6 +370,30 @@ int or_job(const double* x, const double* y, const double* z, const double* edep
   if (n_spheres) *n_spheres = nsph_total;
   free(zs); free(bx); free(by); free(bi); free(hits);
   return 0;
+}
+
+int or_job(const double* x, const double* y, const double* z, const double* edep, int64_t n,
+           double half_length, double d, int zshift_mode, uint32_t n_os, const double* sxsy,
+           const double* edges, int nbins, int sum_mode, int64_t* counts, double* yfy,
+           or_stats* st, or_sphere* spheres_out, int64_t cap, int64_t* n_spheres) {
+  return job_impl(x, y, z, edep, n, half_length, d, zshift_mode, n_os, sxsy, edges, nbins,
+                  sum_mode, counts, yfy, st, spheres_out, cap, n_spheres, 0);
+}
+
+/*
+ * The FP32 geometry variant of or_job (not a reference algorithm: the reference computes in
+ * FP64 throughout and only wishes for a float form, readme.md:29). x, y, the shifts, the box
+ * test in x and y, the x/y lattice index and the sphere distance are computed in float, every
+ * operation rounded on its own; z (box test, lattice index, dz), keys and energies are as in
+ * or_job.
+ */
+int or_job_f32(const double* x, const double* y, const double* z, const double* edep, int64_t n,
+               double half_length, double d, int zshift_mode, uint32_t n_os,
+               const double* sxsy, const double* edges, int nbins, int sum_mode,
+               int64_t* counts, double* yfy, or_stats* st, or_sphere* spheres_out, int64_t cap,
+               int64_t* n_spheres) {
+  return job_impl(x, y, z, edep, n, half_length, d, zshift_mode, n_os, sxsy, edges, nbins,
+                  sum_mode, counts, yfy, st, spheres_out, cap, n_spheres, 1);
 }
 
 /*

@@ -198,6 +198,7 @@ struct st_ctx {
   int64_t spill_budget = 0;   // bytes for the spill tables; 0: 30% of free memory, at most 48 GB
   int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
   int min_chunks = 4;         // ... and kept > min_chunks chunks
+  int precision = 64;         // 32: FP32 geometry variant (x/y geometry in float)
 
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
@@ -327,10 +328,13 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     D.denom = (2. / 3.) * J.g.sphereDiameter;
     D.zsh = J.desc.zshift == ST_ZSHIFT_PLUS ? J.g.scoringRegionHalfLength
           : J.desc.zshift == ST_ZSHIFT_MINUS ? -J.g.scoringRegionHalfLength : 0.0;
-    // with shifts in (-HL', HL'] a deposit at |x| >= 2HL'(1+2^-30) stays outside the voxel;
-    // without shifts (x + 0 = x) the box test itself decides
-    D.xy_keep = J.desc.shift_track ? 2.0 * J.g.scoringRegionHalfLength * (1.0 + 0x1p-30)
-                                   : J.g.scoringRegionHalfLength;
+    // with shifts in (-HL', HL'] a deposit at |x| >= 2HL'(1+2^-30) stays outside the voxel
+    // (2HL'(1+2^-20) when x, the shift and their sum are rounded to float); without shifts
+    // (x + 0 = x) the box test itself decides, and rounding x to float keeps |x| >= HL' outside
+    const bool f32 = c->precision == 32;
+    D.xy_keep = J.desc.shift_track
+                    ? 2.0 * J.g.scoringRegionHalfLength * (1.0 + (f32 ? 0x1p-20 : 0x1p-30))
+                    : J.g.scoringRegionHalfLength;
     D.N = (uint32_t)J.g.numSpheresLinear;
     D.N2 = (uint64_t)D.N * (uint64_t)D.N;
     D.seed = J.desc.seed;
@@ -343,7 +347,16 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
                  D.N >= 128 && D.N < (1u << (st::kCellBits - 2))) ? 1 : 0;
     D.cell_cap = 0;
     D.cell_off = 0;
-    D.cell_size = J.g.sphereDiameter * (1.0 + 0x1p-10);
+    // two hits of one sphere are within d of each other; in the FP32 form within d plus a few
+    // float roundings of coordinates below 4HL' (HL' 2^-16 covers them)
+    D.cell_size = J.g.sphereDiameter * (1.0 + 0x1p-10) +
+                  (f32 ? J.g.scoringRegionHalfLength * 0x1p-16 : 0.0);
+    D.f_HL = (float)J.g.scoringRegionHalfLength;
+    D.f_gSO = (float)J.g.greatestSphereOffset;
+    D.f_d = (float)J.g.sphereDiameter;
+    D.f_inv_d = 1.0f / D.f_d;
+    D.f_r2 = (float)D.r2;
+    D.f_pad = 0.0f;
     if (D.flagged) {
       D.cell_cap = next_pow2((uint64_t)2 * (uint64_t)J.track.n);
       D.cell_off = cells_total;
@@ -465,6 +478,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.PVLO = (unsigned long long*)c->pvlo.p;
   pp.PVHI = (unsigned long long*)c->pvhi.p;
   pp.PKEY = (unsigned long long*)c->pkey.p;
+  pp.fp32 = c->precision == 32 ? 1 : 0;
 
   st::FusedParams& fp = c->cache_fp;
   fp.jobs = pp.jobs;
@@ -492,7 +506,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   fp.unit_table = (int*)c->u_table.p;
   fp.pool_bits = (unsigned int*)c->pool.p;
   fp.chunk_windows = c->chunk_windows;
-  fp.pad2 = 0;
+  fp.fp32 = pp.fp32;
 
   c->cache_blk = blk;
   c->cache_flagged.resize(nj);
@@ -1073,6 +1087,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "max_helpers" && v >= 1 && v <= 4096) c->max_helpers = (int)v;
   else if (n == "share_divisor" && v >= 0 && v <= 1 << 20) c->share_divisor = (int)v;
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
+  else if (n == "precision" && (v == 64 || v == 32)) { c->precision = (int)v; drop_graph(c); }
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
   else if (n == "pipeline_bytes" && v >= 0) c->pipeline_bytes = v > 0 ? v : ((int64_t)1 << 62);
@@ -1091,6 +1106,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "max_helpers") *v = c->max_helpers;
   else if (n == "share_divisor") *v = c->share_divisor;
   else if (n == "shared_min_chunks") *v = c->min_chunks;
+  else if (n == "precision") *v = c->precision;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
   else if (n == "pipeline_bytes") *v = c->pipeline_bytes;

@@ -54,6 +54,13 @@ struct JobDev {
   uint32_t cell_cap;
   int64_t cell_off;
   double cell_size;
+  // FP32 geometry variant: HL', gSO, d, RN(1/d) and r^2 rounded to float (1/d in float)
+  float f_HL;
+  float f_gSO;
+  float f_d;
+  float f_inv_d;
+  float f_r2;
+  float f_pad;
 };
 
 // Deposits are processed in windows of kWindow consecutive kept deposits (one CTA tile of the
@@ -136,7 +143,7 @@ struct FusedParams {
   int* unit_table;            // spill table of the unit (-1 none yet, -2 being acquired)
   unsigned int* pool_bits;    // spill tables in use (one bit per table, gridDim.x tables)
   int32_t chunk_windows;      // windows per chunk
-  int32_t pad2;
+  int32_t fp32;               // 1: FP32 geometry variant (float records, float x/y geometry)
 };
 
 // One slot of the cell hash used for boundary flags: the cell key (EMPTY when free), the
@@ -160,12 +167,13 @@ struct PrepareParams {
   int64_t* blk_offset;        // first kept index of each prepare block inside its job
   CellSlot* cells;            // cell arena (flagged jobs)
   double* PZ;                 // z after the z-origin shift (flagged jobs only)
-  double* PX;
-  double* PY;
-  double* PDZ2;
+  double* PX;                 // FP32 variant: float2 {x, y} per slot
+  double* PY;                 // FP32 variant: unused
+  double* PDZ2;               // FP32 variant: float dz^2 at the slot's float index
   unsigned long long* PVLO;
   unsigned long long* PVHI;
   unsigned long long* PKEY;
+  int32_t fp32;               // 1: records for the FP32 geometry variant
 };
 
 // Device-side planning of the fused kernel's work items from the kept deposit counts.

@@ -237,9 +237,14 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       const int64_t w = k / kWarpTile;
       const int rem = (int)(k - w * kWarpTile);
       const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
-      p.PX[dst] = x;
-      p.PY[dst] = y;
-      p.PDZ2[dst] = st_dmul(dz, dz);
+      if (p.fp32) {
+        reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__double2float_rn(x), __double2float_rn(y));
+        reinterpret_cast<float*>(p.PDZ2)[dst] = __double2float_rn(st_dmul(dz, dz));
+      } else {
+        p.PX[dst] = x;
+        p.PY[dst] = y;
+        p.PDZ2[dst] = st_dmul(dz, dz);
+      }
       uint64_t lo, hi;
       to_fixed(__ddiv_rn(J.edep[i], J.denom), E0, &lo, &hi);
       p.PVLO[dst] = lo;
@@ -266,9 +271,14 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
   const int64_t w = k / kWarpTile;
   const int rem = (int)(k - w * kWarpTile);
   const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
-  p.PX[dst] = __longlong_as_double(0x7FF8000000000000ll);
-  p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
-  p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
+  if (p.fp32) {
+    reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__int_as_float(0x7FC00000), __int_as_float(0x7FC00000));
+    reinterpret_cast<float*>(p.PDZ2)[dst] = __int_as_float(0x7F800000);
+  } else {
+    p.PX[dst] = __longlong_as_double(0x7FF8000000000000ll);
+    p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
+    p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
+  }
   p.PVLO[dst] = 0;
   p.PVHI[dst] = 0;
   p.PKEY[dst] = 0;
@@ -290,7 +300,16 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     const int64_t w = k / kWarpTile;
     const int rem = (int)(k - w * kWarpTile);
     const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
-    const double x = p.PX[dst], y = p.PY[dst], z = p.PZ[dst];
+    double x, y;
+    if (p.fp32) {  // float-rounded x, y: the FP32 jobs' cell size covers the rounding
+      const float2 xy = reinterpret_cast<const float2*>(p.PX)[dst];
+      x = xy.x;
+      y = xy.y;
+    } else {
+      x = p.PX[dst];
+      y = p.PY[dst];
+    }
+    const double z = p.PZ[dst];
     const uint32_t win = (uint32_t)(k / kWindow);
     const CellCoord cc = cell_of(x, y, z, J.cell_size);
     bool boundary = false;
@@ -602,7 +621,9 @@ struct FusedJob {
 // shift, box test, lattice test, key, exact run / warp / shared-memory reduction. For flagged jobs
 // every window ends by binning its complete spheres and moving boundary spheres to G; otherwise
 // spheres accumulate across windows and the shared table spills to G when it fills up.
-template <int CAP, int THREADS>
+// F32: the FP32 geometry variant (x, y, shifts, lattice index and distance in float; z part of
+// the distance, keys and energies as in the FP64 form).
+template <int CAP, int THREADS, bool F32>
 __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob& F,
                                             const SmemTable<CAP>& T, CtaState& cs,
                                             const Spill& G, const BinContext& B, int os,
@@ -616,6 +637,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   shift_uniforms(J.seed, J.track_id, (uint32_t)os, J.shift_track, &ux, &uy);
   const double sx = shift_from_uniform(ux, J.L, J.HL);
   const double sy = shift_from_uniform(uy, J.L, J.HL);
+  const float sxf = __double2float_rn(sx), syf = __double2float_rn(sy);
 
   // a job without window flags whose whole lattice (N^3 spheres) stays below the flush
   // threshold can never need a flush between windows: its windows run without a barrier
@@ -629,6 +651,31 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       const int64_t tb = J.prep_off + w * kWarpTile + lane;
       uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
       unsigned hitmask = 0, boxmask = 0;
+      if constexpr (F32) {
+        // x' = x + sx, box |x'| < HL', a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a,
+        // hit iff (dx^2 + dy^2) + dz^2 <= r^2, every step rounded to float
+        const float2* pxy = reinterpret_cast<const float2*>(P.PX);
+        const float* pdz2 = reinterpret_cast<const float*>(P.PDZ2);
+#pragma unroll
+        for (int p = 0; p < kDepPerLane; ++p) {
+          const float2 xy = __ldg(&pxy[tb + p * 32]);
+          const float x1 = __fadd_rn(xy.x, sxf);
+          const float y1 = __fadd_rn(xy.y, syf);
+          const bool inb = fabsf(x1) < J.f_HL && fabsf(y1) < J.f_HL;
+          boxmask |= (unsigned)inb << p;
+          const float ax = __fsub_rn(x1, J.f_gSO);
+          const float ay = __fsub_rn(y1, J.f_gSO);
+          const int ix = __float2int_rn(__fmul_rn(ax, J.f_inv_d));
+          const int iy = __float2int_rn(__fmul_rn(ay, J.f_inv_d));
+          const float ddx = __fsub_rn(__fmul_rn((float)ix, J.f_d), ax);
+          const float ddy = __fsub_rn(__fmul_rn((float)iy, J.f_d), ay);
+          const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                       __ldg(&pdz2[tb + p * 32]));
+          hitmask |= (unsigned)(inb && dist <= J.f_r2) << p;
+          kxv[p] = (uint32_t)ix;
+          kyv[p] = (uint32_t)iy;
+        }
+      } else {
       // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
 #pragma unroll
       for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
@@ -674,6 +721,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
           kyv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdy[p], kMagic));
         }
       }
+      }
       hits += __popc(hitmask);
       inbox += __popc(boxmask);
       // runs of equal keys inside the lane's consecutive deposits are summed in registers
@@ -686,7 +734,10 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
           const uint64_t lo = __ldg(&P.PVLO[idx]);
           const uint64_t hi = __ldg(&P.PVHI[idx]);
           const uint64_t kzw = __ldg(&P.PKEY[idx]);
-          const uint64_t key = (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N + (kzw & ~kBoundaryBit);
+          // (the FP32 form converts a lattice index like the reference's llrint: sign-extended)
+          const uint64_t key =
+              (F32 ? (uint64_t)(int64_t)(int32_t)kxv[p] + (uint64_t)(int64_t)(int32_t)kyv[p] * J.N
+                   : (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N) + (kzw & ~kBoundaryBit);
           const bool bflag = (kzw & kBoundaryBit) != 0;
           if (key == rkey) {
             add128(rlo, rhi, lo, hi);
@@ -768,7 +819,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
 // oversamples of a small or medium job, one CTA) or helpers of a shared unit (one oversample of
 // a large job, whose window chunks are claimed dynamically by every helper that arrives).
 // ---------------------------------------------------------------------------------------------
-template <int CAP, int THREADS>
+template <int CAP, int THREADS, bool F32>
 __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   static_assert(CAP <= 65536, "used-slot list stores 16-bit slot indices");
   static_assert(THREADS / 32 == kFusedWarps, "a window is one CTA tile of warp tiles");
@@ -880,7 +931,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       if (tid == 0) sG = spill_of(P, t, A.kept);
       __syncthreads();
       const Spill& G = sG;
-      superimpose<CAP, THREADS>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
+      superimpose<CAP, THREADS, F32>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
       const int cnt = F.J.flagged ? 0 : cs.tc[0];  // flagged windows leave the table empty
       bool bin_table;
       if (!shared) {
@@ -1142,32 +1193,48 @@ cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_fl
   return cudaGetLastError();
 }
 
-cudaError_t configure_fused() {
-  cudaError_t e = cudaFuncSetAttribute(k_fused<4096, kFusedThreads>,
+template <bool F32>
+static cudaError_t configure_fused_form() {
+  cudaError_t e = cudaFuncSetAttribute(k_fused<4096, kFusedThreads, F32>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)fused_smem_bytes(4096, kBigHistBins));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fused<8192, kFusedThreads>,
+  return cudaFuncSetAttribute(k_fused<8192, kFusedThreads, F32>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)fused_smem_bytes(8192, kSmallHistBins));
 }
 
+cudaError_t configure_fused() {
+  const cudaError_t e = configure_fused_form<false>();
+  return e != cudaSuccess ? e : configure_fused_form<true>();
+}
+
+template <bool F32>
+static void launch_fused_form(const FusedParams& p, int grid, bool big_table, cudaStream_t s) {
+  if (big_table)
+    k_fused<8192, kFusedThreads, F32>
+        <<<grid, kFusedThreads, fused_smem_bytes(8192, kSmallHistBins), s>>>(p);
+  else
+    k_fused<4096, kFusedThreads, F32>
+        <<<grid, kFusedThreads, fused_smem_bytes(4096, kBigHistBins), s>>>(p);
+}
+
 // Picks the kernel shape: the 8192-slot sphere table when the largest histogram of the batch
 // fits the remaining shared memory (and table_slots does not ask for 4096), else 4096 slots with
-// room for 4096 bins; fills P.smem_hist_bins and P.flush_threshold.
+// room for 4096 bins; fills P.smem_hist_bins and P.flush_threshold. P.fp32 picks the FP32
+// geometry form.
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
-  if (max_nbins <= kSmallHistBins && table_slots != 4096) {
+  const bool big_table = max_nbins <= kSmallHistBins && table_slots != 4096;
+  if (big_table) {
     p.smem_hist_bins = kSmallHistBins;
     p.flush_threshold = 8192 - 4096 - 8192 / 4;  // at most 3/4 full after the next window
-    k_fused<8192, kFusedThreads>
-        <<<grid, kFusedThreads, fused_smem_bytes(8192, kSmallHistBins), s>>>(p);
   } else {
     p.smem_hist_bins = kBigHistBins;
     p.flush_threshold = 4096 / 2;
-    k_fused<4096, kFusedThreads>
-        <<<grid, kFusedThreads, fused_smem_bytes(4096, kBigHistBins), s>>>(p);
   }
+  if (p.fp32) launch_fused_form<true>(p, grid, big_table, s);
+  else launch_fused_form<false>(p, grid, big_table, s);
   return cudaGetLastError();
 }
 

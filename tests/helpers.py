@@ -31,7 +31,7 @@ def gpu_run(ctx, w, mode="batched", export_cap=0, jobs=None, zshift=None, hist_i
     return [o[0] for o in out], [o[1] for o in out], stats, spheres
 
 
-def oracle_run(w, jobs=None, zshift=None, spheres_cap=0, sum_mode=po.OR_SUM_EXACT):
+def oracle_run(w, jobs=None, zshift=None, spheres_cap=0, sum_mode=po.OR_SUM_EXACT, precision=64):
     edges = [po.edges(*h) for h in w.hists]
     counts = [np.zeros(len(e) - 1, dtype=np.int64) for e in edges]
     yfy = [np.zeros(len(e) - 1) for e in edges]
@@ -46,7 +46,7 @@ def oracle_run(w, jobs=None, zshift=None, spheres_cap=0, sum_mode=po.OR_SUM_EXAC
                                   sphere_diameter=float(w.diameter[j]), sxsy=sx,
                                   edges_arr=edges[h], zshift=zshift or w.zshift,
                                   sum_mode=sum_mode, spheres_cap=spheres_cap, counts=counts[h],
-                                  yfy=yfy[h])
+                                  yfy=yfy[h], precision=precision)
         stats.append(s)
         spheres.append(sph)
     return counts, yfy, stats, spheres

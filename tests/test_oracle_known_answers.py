@@ -20,7 +20,7 @@ GOLDEN = json.load(open(os.path.join(HERE, "golden", "known_answers.json")))
 
 
 def run_oracle_case(c, n_os=None, zshift=None, tracks=None, sum_mode=po.OR_SUM_EXACT,
-                    spheres_cap=0):
+                    spheres_cap=0, precision=64):
     kind, nb, lo, hi = c["hist"]
     e = po.edges(kind, nb, lo, hi)
     counts = np.zeros(nb, dtype=np.int64)
@@ -34,7 +34,8 @@ def run_oracle_case(c, n_os=None, zshift=None, tracks=None, sum_mode=po.OR_SUM_E
         _, _, s, sph = po.run_job(*t, half_length=c["half_length"],
                                   sphere_diameter=c["diameter"], sxsy=sx, edges_arr=e,
                                   zshift=zshift or c["zshift"], sum_mode=sum_mode,
-                                  spheres_cap=spheres_cap, counts=counts, yfy=yfy)
+                                  spheres_cap=spheres_cap, counts=counts, yfy=yfy,
+                                  precision=precision)
         stats.append(s)
         spheres.append(sph)
     return e, counts, yfy, stats, spheres
