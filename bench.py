@@ -404,7 +404,7 @@ def ours(args, rank, world):
         spectra = {}
         for prec in (64, 32):
             ctx.set_param("precision", prec)
-            ctx.clear_histograms()
+            ctx.reset_histogram(-1)        # zero every histogram (they stay in place)
             ctx.jobs_reset()
             ctx.run("batched")
             c_ = torch.empty(nb, dtype=torch.int64)

@@ -242,7 +242,9 @@ ST_API st_status st_run_finish(st_ctx* ctx);
 /* The fused kernel of ctx's next run starts only after the fused kernel last enqueued by other
  * (a context on another stream of the same device) has finished; its prepare stage may overlap. */
 ST_API st_status st_ctx_order_after(st_ctx* ctx, const st_ctx* other);
-/* Forgets every histogram of the context (device memory is kept for reuse); ids restart at 0. */
+/* Forgets every histogram of the context (device memory is kept for reuse); ids restart at 0.
+ * Queued jobs that refer to a forgotten histogram make the next run return ST_ERR_STATE (clear
+ * or resubmit them); st_hist_reset(ctx, -1) zeroes every histogram instead. */
 ST_API st_status st_hists_clear(st_ctx* ctx);
 /* Queues n jobs at once (tracks[i] with descs[i]); job_ids may be NULL. */
 ST_API st_status st_job_submit_many(st_ctx* ctx, int32_t n, const st_track_view* tracks,

@@ -278,6 +278,11 @@ st_status upload_host_tracks(st_ctx* c, size_t first, size_t last, int64_t arena
 // [first, last) and the launch parameters; stores them in the context cache.
 st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   const size_t nj = last - first;
+  // a job whose histogram was forgotten (st_hists_clear) has nothing to add into
+  for (size_t j = first; j < last; ++j) {
+    const int32_t h = c->jobs[j].desc.hist_id;
+    if (h < 0 || h >= (int32_t)c->hists.size()) return ST_ERR_STATE;
+  }
   ++c->build_id;
   int64_t prep_total = 0, arena_total = 0, max_pad = 0;
   for (size_t j = first; j < last; ++j) {

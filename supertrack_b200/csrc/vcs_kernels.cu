@@ -415,17 +415,20 @@ template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
                                            const FusedParams& P, const Spill& G, uint64_t key,
                                            uint64_t lo, uint64_t hi, bool boundary, int slot) {
-  // A table of at least two windows' capacity is flushed at window ends once it is a quarter
-  // full (launch_fused), so it never passes three quarters and needs no per-insert check; a
-  // smaller one stops taking new spheres at three quarters (the rest go to the spill table).
+  // A sphere already in the table is always found there. A new sphere that finds the table three
+  // quarters full goes to the spill table instead (the window or oversample then merges the
+  // table into it). Jobs with window flags empty the table at every window end; other jobs keep
+  // their spheres for the whole oversample, and on the 4096-slot table are also flushed at window
+  // ends once it is half full (window_checks).
   constexpr int kHardLimit = (CAP * 3) / 4;
-  if (CAP >= 2 * kWindow || *(volatile int*)&cs->tc[slot] < kHardLimit) {
+  {
     uint32_t h = slot_hash(key, CAP - 1);
 #pragma unroll 1
     for (int probe = 0; probe < 32; ++probe) {
       const uint64_t k = ((volatile uint64_t*)T.keys())[h];
       bool mine = k == key;
       if (!mine && k == kEmptyKey) {
+        if (*(volatile int*)&cs->tc[slot] >= kHardLimit) break;
         const uint64_t old = atomicCAS((unsigned long long*)&T.keys()[h], kEmptyKey, key);
         if (old == kEmptyKey) {
           const int idx = atomicAdd(&cs->tc[slot], 1);
@@ -639,10 +642,12 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   const double sy = shift_from_uniform(uy, J.L, J.HL);
   const float sxf = __double2float_rn(sx), syf = __double2float_rn(sy);
 
-  // a job without window flags whose whole lattice (N^3 spheres) stays below the flush
-  // threshold can never need a flush between windows: its windows run without a barrier
-  const bool window_checks =
-      !J.flagged && (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
+  // Jobs without window flags on the 8192-slot table run their windows without a barrier (a CTA
+  // barrier per window cost more than the occasional new sphere sent to the spill table by a
+  // full table); on the 4096-slot table, a job whose whole lattice (N^3 spheres) exceeds the flush
+  // threshold checks the table at every window end and flushes it to the spill table
+  const bool window_checks = CAP < 2 * kWindow && !J.flagged &&
+                             (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
   int wi = 0;  // window index within this call
   for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps) {
     const int slot = J.flagged ? wi % 3 : 0;
@@ -1228,7 +1233,7 @@ cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots
   const bool big_table = max_nbins <= kSmallHistBins && table_slots != 4096;
   if (big_table) {
     p.smem_hist_bins = kSmallHistBins;
-    p.flush_threshold = 8192 - 4096 - 8192 / 4;  // at most 3/4 full after the next window
+    p.flush_threshold = 8192 - 4096 - 8192 / 4;  // unused: no window checks on this table
   } else {
     p.smem_hist_bins = kBigHistBins;
     p.flush_threshold = 4096 / 2;

@@ -150,3 +150,25 @@ def test_device_resident_tracks(ctx):
     ctx.run()
     hc, _ = ctx.read_histogram(hid2)
     assert np.array_equal(gc, hc) and gc.sum() > 0
+
+
+def test_run_refuses_jobs_of_forgotten_histograms(ctx):
+    """st_hists_clear forgets the histograms; queued jobs that still name one make the run fail
+    with ST_ERR_STATE instead of adding into a stale table. Zeroing (st_hist_reset) keeps them."""
+    ctx.clear()
+    hid = ctx.histogram("lin", 50, 0.01, 100.0)
+    ctx.submit(*_track(3000, seed=3), half_length=100.0, sphere_diameter=5.0, n_oversamples=2,
+               hist=hid, seed=1, track_id=0, zshift="none")
+    ctx.run()
+    first = ctx.read_histogram(hid)[0].copy()
+    assert first.sum() > 0
+    ctx.reset_histogram(-1)
+    ctx.jobs_reset()
+    ctx.run()
+    assert np.array_equal(ctx.read_histogram(hid)[0], first)
+    ctx.clear_histograms()
+    ctx.jobs_reset()
+    with pytest.raises(st.StError) as ei:
+        ctx.run()
+    assert ei.value.status == _capi.ST_ERR_STATE
+    ctx.clear()

@@ -2,7 +2,6 @@
 their spectra (with the CPU oracle standing in for the GPU of each rank), and all-reduce them;
 the result equals the single-process spectrum of all jobs."""
 import os
-import socket
 
 import numpy as np
 import pytest
@@ -24,15 +23,7 @@ def test_lpt_balances_and_covers():
     assert np.array_equal(lpt_assign(costs, 4), lpt_assign(costs, 4))  # deterministic
 
 
-def _free_port():
-    s = socket.socket()
-    s.bind(("127.0.0.1", 0))
-    p = s.getsockname()[1]
-    s.close()
-    return p
-
-
-def _worker(rank, world, port, out_path):
+def _worker(rank, world, store_path, out_path):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
@@ -41,9 +32,9 @@ def _worker(rank, world, port, out_path):
     import pyoracle as po
     import supertrack_b200.workloads as W
     from supertrack_b200.sharding import reduce_spectra, shard
-    os.environ["MASTER_ADDR"] = "127.0.0.1"
-    os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    # rendezvous through a file: no port that another process could take in between
+    dist.init_process_group("gloo", init_method="file://" + store_path, rank=rank,
+                            world_size=world)
     try:
         w = W.config0(n_tracks=12, n_os=3)
         costs = w.sizes * w.n_os
@@ -67,8 +58,8 @@ def test_two_rank_spectrum_equals_single_process(tmp_path):
     import supertrack_b200.workloads as W
     out = str(tmp_path / "r.npz")
     ctx = mp.get_context("spawn")
-    port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    store = str(tmp_path / "store")
+    procs = [ctx.Process(target=_worker, args=(r, 2, store, out)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
