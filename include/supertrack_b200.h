@@ -157,6 +157,10 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   share_divisor      a job runs as shared units (one per oversample) when its kept deposits
  *                      exceed batch units / (share_divisor * grid); 0 = never (default 8)
  *   shared_min_chunks  ... and exceed this many chunks                       (default 4)
+ *   flag_min_kept      a multi-window job on a fine lattice (more than 8192 deposits, at least 4
+ *                      oversamples, 128 or more spheres along an axis) gets window boundary flags
+ *                      when more than this many of its deposits are kept; with fewer, its
+ *                      spheres fit the shared-memory table without them      (default 8192)
  *   precision          64 = the reference's FP64 arithmetic; 32 = FP32 geometry variant: x, y,
  *                      shifts, the x/y box test, x/y lattice index and sphere distance in float
  *                      (z, keys and energies as in FP64). No reference counterpart: the

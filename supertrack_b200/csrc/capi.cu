@@ -199,6 +199,7 @@ struct st_ctx {
   int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
   int min_chunks = 4;         // ... and kept > min_chunks chunks
   int precision = 64;         // 32: FP32 geometry variant (x/y geometry in float)
+  int64_t flag_min_kept = 8192;   // window flags only for jobs with more kept deposits
 
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
@@ -484,6 +485,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.PVHI = (unsigned long long*)c->pvhi.p;
   pp.PKEY = (unsigned long long*)c->pkey.p;
   pp.fp32 = c->precision == 32 ? 1 : 0;
+  pp.flag_min_kept = c->flag_min_kept;
 
   st::FusedParams& fp = c->cache_fp;
   fp.jobs = pp.jobs;
@@ -1093,6 +1095,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "share_divisor" && v >= 0 && v <= 1 << 20) c->share_divisor = (int)v;
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
   else if (n == "precision" && (v == 64 || v == 32)) { c->precision = (int)v; drop_graph(c); }
+  else if (n == "flag_min_kept" && v >= 0) c->flag_min_kept = v;
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
   else if (n == "pipeline_bytes" && v >= 0) c->pipeline_bytes = v > 0 ? v : ((int64_t)1 << 62);
@@ -1112,6 +1115,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "share_divisor") *v = c->share_divisor;
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "precision") *v = c->precision;
+  else if (n == "flag_min_kept") *v = c->flag_min_kept;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
   else if (n == "pipeline_bytes") *v = c->pipeline_bytes;

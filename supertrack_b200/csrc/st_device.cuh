@@ -73,7 +73,8 @@ struct JobAux {
   int32_t e_min;          // min ulp exponent over nonzero contributions
   int32_t e_max;          // max ulp exponent over nonzero contributions
   int32_t flags;          // kAuxNonzero | kAuxNonfinite
-  int32_t pad;
+  int32_t windowed;       // set by k_prep_scan: the job runs with window flags (JobDev::flagged
+                          // and more than PrepareParams::flag_min_kept kept deposits)
   long long kept;              // deposits that can be inside the voxel for some shift
   unsigned long long hits;     // in-sphere deposits summed over all oversamples
   unsigned long long spheres;  // (oversample, sphere) pairs with at least one hit
@@ -174,6 +175,8 @@ struct PrepareParams {
   unsigned long long* PVHI;
   unsigned long long* PKEY;
   int32_t fp32;               // 1: records for the FP32 geometry variant
+  int64_t flag_min_kept;      // a flagged job runs with window flags only above this many kept
+                              // deposits (fewer spheres than that fit the table without them)
 };
 
 // Device-side planning of the fused kernel's work items from the kept deposit counts.

@@ -195,7 +195,10 @@ __global__ void __launch_bounds__(1024) k_prep_scan(PrepareParams p) {
     if (threadIdx.x == 0) s_carry += s_warp[31];
     __syncthreads();
   }
-  if (threadIdx.x == 0) p.aux[j].kept = s_carry;
+  if (threadIdx.x == 0) {
+    p.aux[j].kept = s_carry;
+    p.aux[j].windowed = p.jobs[j].flagged && s_carry > p.flag_min_kept;
+  }
 }
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       p.PVLO[dst] = lo;
       p.PVHI[dst] = hi;
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
-      if (J.flagged) {
+      if (A.windowed) {
         p.PZ[dst] = z1;
         cell_insert(p, J, cell_key(cell_of(x, y, z1, J.cell_size), 0, 0, 0), (uint32_t)(k / kWindow));
       }
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
-  if (!J.flagged) return;
+  if (!p.aux[j].windowed) return;
   const int64_t k0 = p.blk_offset[b];
   const int cnt = p.blk_count[b];
   for (int q = threadIdx.x; q < cnt; q += kPrepThreads) {
@@ -865,6 +868,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     if (A.flags & kAuxNonfinite) continue;  // rejected job: contributes nothing, host reports it
     FusedJob F;
     F.J = P.jobs[W.job];
+    F.J.flagged = A.windowed;  // window flags were computed only for these jobs
     F.E0 = choose_grid_exponent(A.e_min, A.e_max, F.J.n, A.flags & kAuxNonzero);
     F.n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
     const HistDev H = P.hists[F.J.hist];
@@ -1122,7 +1126,7 @@ __global__ void k_reset_aux(JobAux* aux, int n) {
   a.e_min = INT_MAX;
   a.e_max = INT_MIN;
   a.flags = 0;
-  a.pad = 0;
+  a.windowed = 0;
   a.kept = 0;
   a.hits = 0;
   a.spheres = 0;

@@ -127,7 +127,12 @@ def test_window_boundary_flags(ctx, gen, d, n, n_os):
     else:
         w = W.config1(n_tracks=1, n_dep=n, n_os=n_os)
     w.diameter[:] = d
-    gc, gy, gs, _ = gpu_run(ctx, w)
+    old = ctx.get_param("flag_min_kept")
+    ctx.set_param("flag_min_kept", 0)       # flags for every qualifying job, however few kept
+    try:
+        gc, gy, gs, _ = gpu_run(ctx, w)
+    finally:
+        ctx.set_param("flag_min_kept", old)
     oc, oy, os_, _ = oracle_run(w)
     assert_stats_equal(gs, os_)
     assert_hist_equal(gc, gy, oc, oy)
