@@ -399,6 +399,8 @@ struct CtaState {
   int spilled;      // some sphere of this oversample has a partial sum in the spill table
   int ovf[3];       // this window sent a contribution to the spill table directly
   int edges_hist;   // histogram whose edges are in shared memory (-1: none)
+  int log_mode;     // window-flagged private item: window-end spills go to the spill log
+  int logn;         // records in the spill log of this oversample
 };
 
 // Spill table of the current item: the CTA's table restricted to a power-of-two prefix sized
@@ -412,43 +414,68 @@ struct Spill {
   uint32_t cap;
 };
 
-// Adds one sphere contribution to the CTA's shared-memory table, or to the spill table when the
-// shared table is at its load limit or the probe sequence is too long.
+// Appends a sphere's partial sum to the CTA's spill log: the first half of the item's spill table
+// holds (key, lo, hi) records in arrival order, written with plain stores, so a window end does
+// not wait for global atomics. A log takes at most one record per hit of its oversample, and the
+// table has at least two slots per kept deposit, so it cannot run out.
+__device__ __forceinline__ void log_append(CtaState* cs, const FusedParams& P, const Spill& G,
+                                           uint64_t key, uint64_t lo, uint64_t hi) {
+  const unsigned idx = (unsigned)atomicAdd(&cs->logn, 1);
+  if (idx < G.cap / 2) {
+    G.keys[idx] = key;
+    G.lo[idx] = lo;
+    G.hi[idx] = hi;
+  } else {
+    atomicOr(P.error_flags, 1);
+  }
+}
+
+// Adds a contribution to the CTA's shared-memory table. A sphere already in the table is always
+// found there; a new one is refused (false) when the table is three quarters full or its probe
+// sequence is too long.
+template <int CAP>
+__device__ __forceinline__ bool table_insert(const SmemTable<CAP>& T, CtaState* cs, uint64_t key,
+                                             uint64_t lo, uint64_t hi, bool boundary, int slot) {
+  constexpr int kHardLimit = (CAP * 3) / 4;
+  uint32_t h = slot_hash(key, CAP - 1);
+#pragma unroll 1
+  for (int probe = 0; probe < 32; ++probe) {
+    const uint64_t k = ((volatile uint64_t*)T.keys())[h];
+    bool mine = k == key;
+    if (!mine && k == kEmptyKey) {
+      if (*(volatile int*)&cs->tc[slot] >= kHardLimit) return false;
+      const uint64_t old = atomicCAS((unsigned long long*)&T.keys()[h], kEmptyKey, key);
+      if (old == kEmptyKey) {
+        const int idx = atomicAdd(&cs->tc[slot], 1);
+        T.used()[idx] = (uint16_t)h;
+      }
+      mine = old == kEmptyKey || old == key;
+    }
+    if (mine) {
+      acc_add(&T.lo()[h], &T.hi()[h], lo, hi);
+      if (boundary) atomicOr(&T.flags()[h >> 5], 1u << (h & 31));
+      return true;
+    }
+    h = (h + 1) & (CAP - 1);
+  }
+  return false;
+}
+
+// Adds one sphere contribution to the shared-memory table, or, when the table refuses it, to the
+// spill log (window-flagged private items) or the spill table. Jobs with window flags empty the
+// table at every window end; other jobs keep their spheres for the whole oversample, and on the
+// 4096-slot table are also flushed at window ends once it is half full (window_checks).
 template <int CAP>
 __device__ __forceinline__ void sphere_add(const SmemTable<CAP>& T, CtaState* cs,
                                            const FusedParams& P, const Spill& G, uint64_t key,
                                            uint64_t lo, uint64_t hi, bool boundary, int slot) {
-  // A sphere already in the table is always found there. A new sphere that finds the table three
-  // quarters full goes to the spill table instead (the window or oversample then merges the
-  // table into it). Jobs with window flags empty the table at every window end; other jobs keep
-  // their spheres for the whole oversample, and on the 4096-slot table are also flushed at window
-  // ends once it is half full (window_checks).
-  constexpr int kHardLimit = (CAP * 3) / 4;
-  {
-    uint32_t h = slot_hash(key, CAP - 1);
-#pragma unroll 1
-    for (int probe = 0; probe < 32; ++probe) {
-      const uint64_t k = ((volatile uint64_t*)T.keys())[h];
-      bool mine = k == key;
-      if (!mine && k == kEmptyKey) {
-        if (*(volatile int*)&cs->tc[slot] >= kHardLimit) break;
-        const uint64_t old = atomicCAS((unsigned long long*)&T.keys()[h], kEmptyKey, key);
-        if (old == kEmptyKey) {
-          const int idx = atomicAdd(&cs->tc[slot], 1);
-          T.used()[idx] = (uint16_t)h;
-        }
-        mine = old == kEmptyKey || old == key;
-      }
-      if (mine) {
-        acc_add(&T.lo()[h], &T.hi()[h], lo, hi);
-        if (boundary) atomicOr(&T.flags()[h >> 5], 1u << (h & 31));
-        return;
-      }
-      h = (h + 1) & (CAP - 1);
-    }
+  if (table_insert<CAP>(T, cs, key, lo, hi, boundary, slot)) return;
+  *(volatile int*)&cs->ovf[slot] = 1;
+  if (*(volatile int*)&cs->log_mode) {
+    log_append(cs, P, G, key, lo, hi);
+    return;
   }
   *(volatile int*)&cs->spilled = 1;
-  *(volatile int*)&cs->ovf[slot] = 1;
   if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, key, lo, hi))
     atomicOr(P.error_flags, 1);
 }
@@ -617,6 +644,74 @@ __device__ __forceinline__ void bin_spill(const Spill& G, const BinContext& B, c
   }
 }
 
+constexpr int kLogPart = 2048;  // spill-log records per reduction pass (the table holds 8192)
+
+// Partition of a spill-log record: a hash of the key independent of the table's slot hash.
+__device__ __forceinline__ int log_part(uint64_t key, int parts) {
+  return (int)(((uint64_t)(uint32_t)((key * 0xD6E8FEB86659FD93ull) >> 32) * (uint64_t)parts) >> 32);
+}
+
+// End of a window-flagged private oversample: sums the spill log per sphere and bins it. The
+// records are taken in hash partitions of about kLogPart, each summed in the (empty) shared table
+// and binned; a partition in which the table refused a record goes whole to a hash table in the
+// second half of the spill table instead, which is binned last, so no sphere is split between
+// the two. The log records are cleared for the pool's next user.
+template <int CAP, int THREADS>
+__device__ __forceinline__ void log_reduce(const SmemTable<CAP>& T, CtaState& cs,
+                                           const FusedParams& P, const Spill& G,
+                                           const BinContext& B, unsigned int& spheres,
+                                           unsigned int& binned, int os) {
+  const int tid = threadIdx.x;
+  const int L = cs.logn;  // read after superimpose's closing barrier: the same in every thread
+  if (L == 0) return;
+  Spill H = G;            // fallback hash table: the second half of the spill table
+  H.keys += G.cap / 2;
+  H.lo += G.cap / 2;
+  H.hi += G.cap / 2;
+  H.cap = G.cap / 2;
+  const int parts = (L + kLogPart - 1) / kLogPart;
+  if (tid == 0) for (int k = 0; k < 3; ++k) cs.tc[k] = 0;
+  __syncthreads();
+  int any_out = 0;
+  for (int part = 0; part < parts; ++part) {
+    const int slot = part % 3;
+    int refused = 0;
+    for (int i = tid; i < L; i += THREADS) {
+      const uint64_t key = __ldcg((const unsigned long long*)&G.keys[i]);
+      if (log_part(key, parts) != part) continue;
+      if (!table_insert<CAP>(T, &cs, key, __ldcg(&G.lo[i]), __ldcg(&G.hi[i]), false, slot)) {
+        if (!gtable_add(H.keys, H.lo, H.hi, H.used, H.count, H.cap, key, __ldcg(&G.lo[i]),
+                        __ldcg(&G.hi[i])))
+          atomicOr(P.error_flags, 1);
+        refused = 1;
+      }
+    }
+    refused = __syncthreads_or(refused);
+    const int cnt = cs.tc[slot];
+    if (tid == 0) cs.tc[(part + 1) % 3] = 0;  // the next pass's slot: last read two passes ago
+    for (int i = tid; i < cnt; i += THREADS) {
+      const uint32_t h = T.used()[i];
+      if (refused) {
+        if (!gtable_add(H.keys, H.lo, H.hi, H.used, H.count, H.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
+          atomicOr(P.error_flags, 1);
+      } else {
+        bin_sphere(B, P, T.keys()[h], T.lo()[h], T.hi()[h], spheres, binned, os);
+      }
+      T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
+    }
+    any_out |= refused;
+    __syncthreads();
+  }
+  for (int i = tid; i < L; i += THREADS) { G.keys[i] = kEmptyKey; G.lo[i] = 0; G.hi[i] = 0; }
+  if (any_out) bin_spill<THREADS>(H, B, P, spheres, binned, os);
+  __syncthreads();
+  if (tid == 0) {
+    for (int k = 0; k < 3; ++k) cs.tc[k] = 0;
+    cs.logn = 0;
+  }
+  __syncthreads();
+}
+
 struct FusedJob {
   JobDev J;
   int E0;
@@ -649,6 +744,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   // barrier per window cost more than the occasional new sphere sent to the spill table by a
   // full table); on the 4096-slot table, a job whose whole lattice (N^3 spheres) exceeds the flush
   // threshold checks the table at every window end and flushes it to the spill table
+  const bool log_mode = cs.log_mode != 0;
   const bool window_checks = CAP < 2 * kWindow && !J.flagged &&
                              (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
   int wi = 0;  // window index within this call
@@ -796,7 +892,9 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         const bool flagged = (T.flags()[h >> 5] & bit) != 0;
         if (flagged) atomicAnd(&T.flags()[h >> 5], ~bit);
         const bool out = all_out || flagged;
-        if (out) {
+        if (out && log_mode) {
+          log_append(&cs, P, G, T.keys()[h], T.lo()[h], T.hi()[h]);
+        } else if (out) {
           if (!gtable_add(G.keys, G.lo, G.hi, G.used, G.count, G.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
             atomicOr(P.error_flags, 1);
           sent = 1;
@@ -851,6 +949,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
   if (tid == 0) {
     for (int k = 0; k < 3; ++k) { cs.tc[k] = 0; cs.ovf[k] = 0; }
     cs.spilled = 0;
+    cs.log_mode = 0;
+    cs.logn = 0;
     cs.edges_hist = -1;
   }
   __syncthreads();
@@ -937,10 +1037,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
         wb = (int64_t)c * wpc;
         we = wb + wpc < F.n_wt ? wb + wpc : F.n_wt;
       }
-      if (tid == 0) sG = spill_of(P, t, A.kept);
+      if (tid == 0) {
+        sG = spill_of(P, t, A.kept);
+        cs.log_mode = F.J.flagged && !shared;  // a single CTA sees every window of the oversample
+      }
       __syncthreads();
       const Spill& G = sG;
       superimpose<CAP, THREADS, F32>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
+      if (cs.log_mode) log_reduce<CAP, THREADS>(T, cs, P, G, B, spheres, binned, os);
       const int cnt = F.J.flagged ? 0 : cs.tc[0];  // flagged windows leave the table empty
       bool bin_table;
       if (!shared) {
@@ -975,6 +1079,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       if (tid == 0) {
         for (int k = 0; k < 3; ++k) { cs.tc[k] = 0; cs.ovf[k] = 0; }
         cs.spilled = 0;
+        cs.log_mode = 0;
       }
       __syncthreads();
     }
