@@ -644,18 +644,70 @@ __device__ __forceinline__ void bin_spill(const Spill& G, const BinContext& B, c
   }
 }
 
-constexpr int kLogPart = 2048;  // spill-log records per reduction pass (the table holds 8192)
-
 // Partition of a spill-log record: a hash of the key independent of the table's slot hash.
 __device__ __forceinline__ int log_part(uint64_t key, int parts) {
   return (int)(((uint64_t)(uint32_t)((key * 0xD6E8FEB86659FD93ull) >> 32) * (uint64_t)parts) >> 32);
 }
 
-// End of a window-flagged private oversample: sums the spill log per sphere and bins it. The
-// records are taken in hash partitions of about kLogPart, each summed in the (empty) shared table
-// and binned; a partition in which the table refused a record goes whole to a hash table in the
-// second half of the spill table instead, which is binned last, so no sphere is split between
-// the two. The log records are cleared for the pool's next user.
+// One reduction pass: the records [r0, r1) of R whose partition is `part` (all of them when
+// parts is 1) are summed in the empty shared table and binned. If the table refused any record,
+// the pass's spheres go whole to the hash table F instead (binned last), so that no sphere is
+// split between the two. Returns whether F received anything (the same in every thread).
+template <int CAP, int THREADS>
+__device__ __forceinline__ int log_pass(const SmemTable<CAP>& T, CtaState& cs,
+                                        const FusedParams& P, const Spill& R, int r0, int r1,
+                                        int part, int parts, const Spill& F, int slot,
+                                        const BinContext& B, unsigned int& spheres,
+                                        unsigned int& binned, int os) {
+  const int tid = threadIdx.x;
+  int refused = 0;
+  // four records in flight per thread before any is inserted
+  for (int i0 = r0 + tid; i0 < r1; i0 += 4 * THREADS) {
+    uint64_t kk[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * THREADS;
+      kk[u] = i < r1 ? __ldcg((const unsigned long long*)&R.keys[i]) : kEmptyKey;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * THREADS;
+      if (i >= r1 || (parts > 1 && log_part(kk[u], parts) != part)) continue;
+      const uint64_t lo = __ldcg(&R.lo[i]), hi = __ldcg(&R.hi[i]);
+      if (!table_insert<CAP>(T, &cs, kk[u], lo, hi, false, slot)) {
+        if (!gtable_add(F.keys, F.lo, F.hi, F.used, F.count, F.cap, kk[u], lo, hi))
+          atomicOr(P.error_flags, 1);
+        refused = 1;
+      }
+    }
+  }
+  refused = __syncthreads_or(refused);
+  const int cnt = cs.tc[slot];
+  if (tid == 0) cs.tc[(slot + 1) % 3] = 0;  // the next pass's slot: last read two passes ago
+  for (int i = tid; i < cnt; i += THREADS) {
+    const uint32_t h = T.used()[i];
+    if (refused) {
+      if (!gtable_add(F.keys, F.lo, F.hi, F.used, F.count, F.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
+        atomicOr(P.error_flags, 1);
+    } else {
+      bin_sphere(B, P, T.keys()[h], T.lo()[h], T.hi()[h], spheres, binned, os);
+    }
+    T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
+  }
+  __syncthreads();
+  return refused;
+}
+
+// End of a window-flagged private oversample: sums the spill log (the first half of the spill
+// table, records [0, L)) per sphere and bins it, in passes of at most CAP / 2 records (a pass has
+// no more distinct keys than records, so the table stays at most half full).
+//  - Bucketed (more than one pass, and the per-pass counts fit the table's used-slot list, free at
+//    this point): the records are counted per hash partition, scattered into buckets in the second
+//    half of the spill table, and each bucket is summed in one pass; the emptied first half is the
+//    fallback table, and the bucket bounds sit in the spill table's used list beyond its reach.
+//  - Otherwise every pass scans the whole log for its partition, with the second half of the
+//    spill table as the fallback.
+// Every record is cleared again for the pool's next user.
 template <int CAP, int THREADS>
 __device__ __forceinline__ void log_reduce(const SmemTable<CAP>& T, CtaState& cs,
                                            const FusedParams& P, const Spill& G,
@@ -664,46 +716,59 @@ __device__ __forceinline__ void log_reduce(const SmemTable<CAP>& T, CtaState& cs
   const int tid = threadIdx.x;
   const int L = cs.logn;  // read after superimpose's closing barrier: the same in every thread
   if (L == 0) return;
-  Spill H = G;            // fallback hash table: the second half of the spill table
-  H.keys += G.cap / 2;
-  H.lo += G.cap / 2;
-  H.hi += G.cap / 2;
-  H.cap = G.cap / 2;
-  const int parts = (L + kLogPart - 1) / kLogPart;
+  constexpr int kPart = CAP / 2;  // records per pass
+  const int parts = (L + kPart - 1) / kPart;
+  Spill lo_half = G, hi_half = G;
+  lo_half.cap = G.cap / 2;
+  hi_half.keys += G.cap / 2;
+  hi_half.lo += G.cap / 2;
+  hi_half.hi += G.cap / 2;
+  hi_half.cap = G.cap / 2;
   if (tid == 0) for (int k = 0; k < 3; ++k) cs.tc[k] = 0;
   __syncthreads();
   int any_out = 0;
-  for (int part = 0; part < parts; ++part) {
-    const int slot = part % 3;
-    int refused = 0;
+  if (parts == 1 || 2 * parts > CAP / 2) {
+    for (int q = 0; q < parts; ++q)
+      any_out |= log_pass<CAP, THREADS>(T, cs, P, lo_half, 0, L, q, parts, hi_half, q % 3, B,
+                                        spheres, binned, os);
+    for (int i = tid; i < L; i += THREADS) { G.keys[i] = kEmptyKey; G.lo[i] = 0; G.hi[i] = 0; }
+    if (any_out) bin_spill<THREADS>(hi_half, B, P, spheres, binned, os);
+  } else {
+    unsigned int* cnt = reinterpret_cast<unsigned int*>(T.used());  // parts counts, parts cursors
+    uint32_t* bounds = G.used + G.cap / 2;                              // parts + 1 bucket bounds
+    for (int i = tid; i < 2 * parts; i += THREADS) cnt[i] = 0;
+    __syncthreads();
+    for (int i = tid; i < L; i += THREADS)
+      atomicAdd(&cnt[log_part(__ldcg((const unsigned long long*)&G.keys[i]), parts)], 1u);
+    __syncthreads();
+    if (tid == 0) {
+      unsigned run = 0;
+      for (int q = 0; q < parts; ++q) {
+        bounds[q] = run;
+        cnt[parts + q] = run;
+        run += cnt[q];
+      }
+      bounds[parts] = run;
+    }
+    __syncthreads();
     for (int i = tid; i < L; i += THREADS) {
       const uint64_t key = __ldcg((const unsigned long long*)&G.keys[i]);
-      if (log_part(key, parts) != part) continue;
-      if (!table_insert<CAP>(T, &cs, key, __ldcg(&G.lo[i]), __ldcg(&G.hi[i]), false, slot)) {
-        if (!gtable_add(H.keys, H.lo, H.hi, H.used, H.count, H.cap, key, __ldcg(&G.lo[i]),
-                        __ldcg(&G.hi[i])))
-          atomicOr(P.error_flags, 1);
-        refused = 1;
-      }
+      const uint64_t lo = __ldcg(&G.lo[i]), hi = __ldcg(&G.hi[i]);
+      const unsigned pos = atomicAdd(&cnt[parts + log_part(key, parts)], 1u);
+      hi_half.keys[pos] = key; hi_half.lo[pos] = lo; hi_half.hi[pos] = hi;
+      G.keys[i] = kEmptyKey; G.lo[i] = 0; G.hi[i] = 0;
     }
-    refused = __syncthreads_or(refused);
-    const int cnt = cs.tc[slot];
-    if (tid == 0) cs.tc[(part + 1) % 3] = 0;  // the next pass's slot: last read two passes ago
-    for (int i = tid; i < cnt; i += THREADS) {
-      const uint32_t h = T.used()[i];
-      if (refused) {
-        if (!gtable_add(H.keys, H.lo, H.hi, H.used, H.count, H.cap, T.keys()[h], T.lo()[h], T.hi()[h]))
-          atomicOr(P.error_flags, 1);
-      } else {
-        bin_sphere(B, P, T.keys()[h], T.lo()[h], T.hi()[h], spheres, binned, os);
-      }
-      T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
+    __syncthreads();  // buckets written, the first half empty again (the fallback from here on)
+    for (int q = 0; q < parts; ++q) {
+      const int r0 = (int)__ldcg(&bounds[q]), r1 = (int)__ldcg(&bounds[q + 1]);
+      any_out |= log_pass<CAP, THREADS>(T, cs, P, hi_half, r0, r1, q, 1, lo_half, q % 3, B,
+                                        spheres, binned, os);
     }
-    any_out |= refused;
-    __syncthreads();
+    for (int i = tid; i < L; i += THREADS) {
+      hi_half.keys[i] = kEmptyKey; hi_half.lo[i] = 0; hi_half.hi[i] = 0;
+    }
+    if (any_out) bin_spill<THREADS>(lo_half, B, P, spheres, binned, os);
   }
-  for (int i = tid; i < L; i += THREADS) { G.keys[i] = kEmptyKey; G.lo[i] = 0; G.hi[i] = 0; }
-  if (any_out) bin_spill<THREADS>(H, B, P, spheres, binned, os);
   __syncthreads();
   if (tid == 0) {
     for (int k = 0; k < 3; ++k) cs.tc[k] = 0;
