@@ -25,6 +25,14 @@ __device__ __forceinline__ uint32_t slot_hash(uint64_t key, uint32_t mask) {
   return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 40) & mask;
 }
 
+// Slot of a sphere key in the shared-memory table: Fibonacci hashing proper, the top
+// log2(mask + 1) bits of key * 2^64/phi (mask + 1 a power of two of at least 2). The middle bits
+// that slot_hash takes map the regular lattice keys of a straight track into long runs of
+// neighbouring slots, which at a quarter load already exceeded the 32-slot probe limit.
+__device__ __forceinline__ uint32_t table_hash(uint64_t key, uint32_t mask) {
+  return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 32) >> __clz((int)mask);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Lattice index along one axis, k = llrint(a / d), bit-exact with the IEEE quotient. The fused
 // kernel forms q = RN(a * RN(1/d)), whose distance to RN(a/d) is below |q| * 2^-51.2; it takes
@@ -399,7 +407,7 @@ struct CtaState {
   int spilled;      // some sphere of this oversample has a partial sum in the spill table
   int ovf[3];       // this window sent a contribution to the spill table directly
   int edges_hist;   // histogram whose edges are in shared memory (-1: none)
-  int log_mode;     // window-flagged private item: window-end spills go to the spill log
+  int log_mode;     // private item: table overflows, flushes and window-end spills go to the log
   int logn;         // records in the spill log of this oversample
 };
 
@@ -437,7 +445,7 @@ template <int CAP>
 __device__ __forceinline__ bool table_insert(const SmemTable<CAP>& T, CtaState* cs, uint64_t key,
                                              uint64_t lo, uint64_t hi, bool boundary, int slot) {
   constexpr int kHardLimit = (CAP * 3) / 4;
-  uint32_t h = slot_hash(key, CAP - 1);
+  uint32_t h = table_hash(key, CAP - 1);
 #pragma unroll 1
   for (int probe = 0; probe < 32; ++probe) {
     const uint64_t k = ((volatile uint64_t*)T.keys())[h];
@@ -549,6 +557,17 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
     } else {
       atomicOr(P.error_flags, 2);
     }
+  }
+}
+
+// Appends every shared-memory entry to the spill log and empties the shared table.
+template <int CAP, int THREADS>
+__device__ __forceinline__ void flush_to_log(const SmemTable<CAP>& T, int cnt, CtaState* cs,
+                                             const FusedParams& P, const Spill& G) {
+  for (int i = threadIdx.x; i < cnt; i += THREADS) {
+    const uint32_t h = T.used()[i];
+    log_append(cs, P, G, T.keys()[h], T.lo()[h], T.hi()[h]);
+    T.keys()[h] = kEmptyKey; T.lo()[h] = 0; T.hi()[h] = 0;
   }
 }
 
@@ -974,9 +993,10 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
     } else if (window_checks && wt0 + kWarps < wt_end) {
       __syncthreads();
       if (cs.tc[0] > P.flush_threshold) {
-        flush_to_spill<CAP, THREADS>(T, cs.tc[0], P, G);
+        if (log_mode) flush_to_log<CAP, THREADS>(T, cs.tc[0], &cs, P, G);
+        else flush_to_spill<CAP, THREADS>(T, cs.tc[0], P, G);
         __syncthreads();
-        if (tid == 0) { cs.tc[0] = 0; cs.spilled = 1; }
+        if (tid == 0) { cs.tc[0] = 0; cs.spilled |= !log_mode; }
         __syncthreads();
       }
     }
@@ -1104,12 +1124,21 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       }
       if (tid == 0) {
         sG = spill_of(P, t, A.kept);
-        cs.log_mode = F.J.flagged && !shared;  // a single CTA sees every window of the oversample
+        cs.log_mode = !shared;  // a single CTA sees every window of the oversample
       }
       __syncthreads();
       const Spill& G = sG;
       superimpose<CAP, THREADS, F32>(P, F, T, cs, G, B, os, wb, we, hits, inbox, spheres, binned);
-      if (cs.log_mode) log_reduce<CAP, THREADS>(T, cs, P, G, B, spheres, binned, os);
+      if (cs.log_mode) {
+        if (!F.J.flagged && cs.logn > 0) {
+          // the table's spheres may have parts in the log: they join it
+          flush_to_log<CAP, THREADS>(T, cs.tc[0], &cs, P, G);
+          __syncthreads();
+          if (tid == 0) cs.tc[0] = 0;
+          __syncthreads();
+        }
+        log_reduce<CAP, THREADS>(T, cs, P, G, B, spheres, binned, os);
+      }
       const int cnt = F.J.flagged ? 0 : cs.tc[0];  // flagged windows leave the table empty
       bool bin_table;
       if (!shared) {
