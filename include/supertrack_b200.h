@@ -152,7 +152,7 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
 /* Named work-planning parameters (all take effect at the next run):
  *   item_cost          deposit*oversamples per private work item            (default 262144)
  *   grid               resident CTAs of the fused kernel, 0 = one per SM     (default 0)
- *   chunk_windows      windows of 4096 kept deposits per chunk of a shared unit   (default 4)
+ *   chunk_windows      windows of 8192 kept deposits per chunk of a shared unit   (default 4)
  *   max_helpers        helper items per shared unit                          (default 32)
  *   share_divisor      a job runs as shared units (one per oversample) when its kept deposits
  *                      exceed batch units / (share_divisor * grid); 0 = never (default 8)

@@ -193,7 +193,7 @@ struct st_ctx {
   int64_t cache_units = 0;
   int64_t cache_item_cap = 0;
   st::PlanParams cache_plan{};
-  int chunk_windows = 4;      // windows (4096 deposits each) per chunk of a shared unit
+  int chunk_windows = 4;      // windows (8192 deposits each) per chunk of a shared unit
   int max_helpers = 32;       // helper items per shared unit
   int64_t spill_budget = 0;   // bytes for the spill tables; 0: 30% of free memory, at most 48 GB
   int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
@@ -349,7 +349,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     D.shift_track = J.desc.shift_track ? 1 : 0;
     D.hist = J.desc.hist_id;
     // boundary flags pay off for multi-window jobs on fine lattices with several oversamples
-    D.flagged = (J.track.n > 2 * st::kWindow && J.desc.n_oversamples >= 4 &&
+    D.flagged = (J.track.n > 2 * st::kCtaTile && J.desc.n_oversamples >= 4 &&
                  D.N >= 128 && D.N < (1u << (st::kCellBits - 2))) ? 1 : 0;
     D.cell_cap = 0;
     D.cell_off = 0;

@@ -184,7 +184,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   D.n_os = (int32_t)desc->n_oversamples;
   D.shift_track = desc->shift_track ? 1 : 0;
   D.hist = 0;
-  D.flagged = (n > 2 * st::kWindow && desc->n_oversamples >= 4 && D.N >= 128 &&
+  D.flagged = (n > 2 * st::kCtaTile && desc->n_oversamples >= 4 && D.N >= 128 &&
                D.N < (1u << (st::kCellBits - 2))) ? 1 : 0;
   D.cell_cap = kNaCellCap;
   D.cell_off = 0;

@@ -63,8 +63,8 @@ struct JobDev {
   float f_pad;
 };
 
-// Deposits are processed in windows of kWindow consecutive kept deposits (one CTA tile of the
-// fused kernel). A kept deposit is a boundary deposit when a kept deposit of another window lies
+// Deposits are processed in windows of kWindow consecutive kept deposits (two warp tiles per warp
+// of the fused kernel's CTA). A kept deposit is a boundary deposit when a kept deposit of another window lies
 // within distance d of it; the flag travels in bit 63 of its PKEY word (keys are below 2^63).
 constexpr unsigned long long kBoundaryBit = 1ull << 63;
 
@@ -211,7 +211,9 @@ struct PlanParams {
 constexpr int kPrepThreads = 256;
 constexpr int kPrepSlotsPerBlock = 1024;                // source deposits per prepare block
 constexpr int kFusedWarps = 32;                       // warps of the fused kernel's CTA
-constexpr int kWindow = kFusedWarps * kWarpTile;      // kept deposits per window
+constexpr int kCtaTile = kFusedWarps * kWarpTile;    // kept deposits of one warp tile per warp
+constexpr int kWinTiles = 2;                          // warp tiles per warp in a window
+constexpr int kWindow = kWinTiles * kCtaTile;         // kept deposits per window (8192)
 constexpr int kCellBits = 21;                         // bits per axis of a cell key
 
 }  // namespace st

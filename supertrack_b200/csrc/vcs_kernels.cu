@@ -829,134 +829,138 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   // full table); on the 4096-slot table, a job whose whole lattice (N^3 spheres) exceeds the flush
   // threshold checks the table at every window end and flushes it to the spill table
   const bool log_mode = cs.log_mode != 0;
-  const bool window_checks = CAP < 2 * kWindow && !J.flagged &&
+  const bool window_checks = CAP < 2 * kCtaTile && !J.flagged &&
                              (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
   int wi = 0;  // window index within this call
-  for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps) {
+  for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps * kWinTiles) {
     const int slot = J.flagged ? wi % 3 : 0;
-    const int64_t w = wt0 + warp;
-    if (w < wt_end) {
-      const int64_t tb = J.prep_off + w * kWarpTile + lane;
-      uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
-      unsigned hitmask = 0, boxmask = 0;
-      if constexpr (F32) {
-        // x' = x + sx, box |x'| < HL', a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a,
-        // hit iff (dx^2 + dy^2) + dz^2 <= r^2, every step rounded to float
-        const float2* pxy = reinterpret_cast<const float2*>(P.PX);
-        const float* pdz2 = reinterpret_cast<const float*>(P.PDZ2);
-#pragma unroll
-        for (int p = 0; p < kDepPerLane; ++p) {
-          const float2 xy = __ldg(&pxy[tb + p * 32]);
-          const float x1 = __fadd_rn(xy.x, sxf);
-          const float y1 = __fadd_rn(xy.y, syf);
-          const bool inb = fabsf(x1) < J.f_HL && fabsf(y1) < J.f_HL;
-          boxmask |= (unsigned)inb << p;
-          const float ax = __fsub_rn(x1, J.f_gSO);
-          const float ay = __fsub_rn(y1, J.f_gSO);
-          const int ix = __float2int_rn(__fmul_rn(ax, J.f_inv_d));
-          const int iy = __float2int_rn(__fmul_rn(ay, J.f_inv_d));
-          const float ddx = __fsub_rn(__fmul_rn((float)ix, J.f_d), ax);
-          const float ddy = __fsub_rn(__fmul_rn((float)iy, J.f_d), ay);
-          const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
-                                       __ldg(&pdz2[tb + p * 32]));
-          hitmask |= (unsigned)(inb && dist <= J.f_r2) << p;
-          kxv[p] = (uint32_t)ix;
-          kyv[p] = (uint32_t)iy;
-        }
-      } else {
-      // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
-#pragma unroll
-      for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
-        double ax[kGeoBlock], ay[kGeoBlock], kdx[kGeoBlock], kdy[kGeoBlock];
-        unsigned risk = 0;
-#pragma unroll
-        for (int p = 0; p < kGeoBlock; ++p) {
-          const double x1 = st_dadd(__ldg(&P.PX[tb + (h4 + p) * 32]), sx);
-          const double y1 = st_dadd(__ldg(&P.PY[tb + (h4 + p) * 32]), sy);
-          const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
-          boxmask |= (unsigned)inb << (h4 + p);
-          ax[p] = st_dsub(x1, J.gSO);
-          ay[p] = st_dsub(y1, J.gSO);
-          const double qx = st_dmul(ax[p], J.inv_d);
-          const double qy = st_dmul(ay[p], J.inv_d);
-          kdx[p] = st_dsub(st_dadd(qx, kMagic), kMagic);
-          kdy[p] = st_dsub(st_dadd(qy, kMagic), kMagic);
-          const bool near_half = fabs(st_dsub(qx, kdx[p])) >= kRiskBand ||
-                                 fabs(st_dsub(qy, kdy[p])) >= kRiskBand;
-          risk |= (unsigned)(near_half && inb) << p;
-        }
-        if (risk) {
-          // q = RN(a * RN(1/d)) is within |q| 2^-51.2 of RN(a/d), far below 2^-20 for in-box
-          // quotients (|q| < 2^21); only a quotient this close to a half-integer can round
-          // differently, and then the IEEE division decides (rare: lattice-aligned inputs)
-#pragma unroll
+    // a window is kWinTiles warp tiles per warp
+#pragma unroll 1
+    for (int tt = 0; tt < kWinTiles; ++tt) {
+      const int64_t w = wt0 + tt * kWarps + warp;
+      if (w < wt_end) {
+        const int64_t tb = J.prep_off + w * kWarpTile + lane;
+        uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
+        unsigned hitmask = 0, boxmask = 0;
+        if constexpr (F32) {
+          // x' = x + sx, box |x'| < HL', a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a,
+          // hit iff (dx^2 + dy^2) + dz^2 <= r^2, every step rounded to float
+          const float2* pxy = reinterpret_cast<const float2*>(P.PX);
+          const float* pdz2 = reinterpret_cast<const float*>(P.PDZ2);
+  #pragma unroll
+          for (int p = 0; p < kDepPerLane; ++p) {
+            const float2 xy = __ldg(&pxy[tb + p * 32]);
+            const float x1 = __fadd_rn(xy.x, sxf);
+            const float y1 = __fadd_rn(xy.y, syf);
+            const bool inb = fabsf(x1) < J.f_HL && fabsf(y1) < J.f_HL;
+            boxmask |= (unsigned)inb << p;
+            const float ax = __fsub_rn(x1, J.f_gSO);
+            const float ay = __fsub_rn(y1, J.f_gSO);
+            const int ix = __float2int_rn(__fmul_rn(ax, J.f_inv_d));
+            const int iy = __float2int_rn(__fmul_rn(ay, J.f_inv_d));
+            const float ddx = __fsub_rn(__fmul_rn((float)ix, J.f_d), ax);
+            const float ddy = __fsub_rn(__fmul_rn((float)iy, J.f_d), ay);
+            const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                         __ldg(&pdz2[tb + p * 32]));
+            hitmask |= (unsigned)(inb && dist <= J.f_r2) << p;
+            kxv[p] = (uint32_t)ix;
+            kyv[p] = (uint32_t)iy;
+          }
+        } else {
+        // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
+  #pragma unroll
+        for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
+          double ax[kGeoBlock], ay[kGeoBlock], kdx[kGeoBlock], kdy[kGeoBlock];
+          unsigned risk = 0;
+  #pragma unroll
           for (int p = 0; p < kGeoBlock; ++p) {
-            if (risk & (1u << p)) {
-              kdx[p] = rint(__ddiv_rn(ax[p], J.d));
-              kdy[p] = rint(__ddiv_rn(ay[p], J.d));
+            const double x1 = st_dadd(__ldg(&P.PX[tb + (h4 + p) * 32]), sx);
+            const double y1 = st_dadd(__ldg(&P.PY[tb + (h4 + p) * 32]), sy);
+            const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
+            boxmask |= (unsigned)inb << (h4 + p);
+            ax[p] = st_dsub(x1, J.gSO);
+            ay[p] = st_dsub(y1, J.gSO);
+            const double qx = st_dmul(ax[p], J.inv_d);
+            const double qy = st_dmul(ay[p], J.inv_d);
+            kdx[p] = st_dsub(st_dadd(qx, kMagic), kMagic);
+            kdy[p] = st_dsub(st_dadd(qy, kMagic), kMagic);
+            const bool near_half = fabs(st_dsub(qx, kdx[p])) >= kRiskBand ||
+                                   fabs(st_dsub(qy, kdy[p])) >= kRiskBand;
+            risk |= (unsigned)(near_half && inb) << p;
+          }
+          if (risk) {
+            // q = RN(a * RN(1/d)) is within |q| 2^-51.2 of RN(a/d), far below 2^-20 for in-box
+            // quotients (|q| < 2^21); only a quotient this close to a half-integer can round
+            // differently, and then the IEEE division decides (rare: lattice-aligned inputs)
+  #pragma unroll
+            for (int p = 0; p < kGeoBlock; ++p) {
+              if (risk & (1u << p)) {
+                kdx[p] = rint(__ddiv_rn(ax[p], J.d));
+                kdy[p] = rint(__ddiv_rn(ay[p], J.d));
+              }
+            }
+          }
+  #pragma unroll
+          for (int p = 0; p < kGeoBlock; ++p) {
+            const double ddx = st_dsub(st_dmul(kdx[p], J.d), ax[p]);
+            const double ddy = st_dsub(st_dmul(kdy[p], J.d), ay[p]);
+            const double dz2 = __ldg(&P.PDZ2[tb + (h4 + p) * 32]);
+            const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dz2);
+            const bool hit = ((boxmask >> (h4 + p)) & 1u) && dist <= J.r2;
+            hitmask |= (unsigned)hit << (h4 + p);
+            kxv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdx[p], kMagic));
+            kyv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdy[p], kMagic));
+          }
+        }
+        }
+        hits += __popc(hitmask);
+        inbox += __popc(boxmask);
+        // runs of equal keys inside the lane's consecutive deposits are summed in registers
+        uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
+        bool rflag = false;
+  #pragma unroll
+        for (int p = 0; p < kDepPerLane; ++p) {
+          if (hitmask & (1u << p)) {
+            const int64_t idx = tb + p * 32;
+            const uint64_t lo = __ldg(&P.PVLO[idx]);
+            const uint64_t hi = __ldg(&P.PVHI[idx]);
+            const uint64_t kzw = __ldg(&P.PKEY[idx]);
+            // (the FP32 form converts a lattice index like the reference's llrint: sign-extended)
+            const uint64_t key =
+                (F32 ? (uint64_t)(int64_t)(int32_t)kxv[p] + (uint64_t)(int64_t)(int32_t)kyv[p] * J.N
+                     : (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N) + (kzw & ~kBoundaryBit);
+            const bool bflag = (kzw & kBoundaryBit) != 0;
+            if (key == rkey) {
+              add128(rlo, rhi, lo, hi);
+              rflag |= bflag;
+            } else {
+              if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
+              rkey = key; rlo = lo; rhi = hi; rflag = bflag;
             }
           }
         }
-#pragma unroll
-        for (int p = 0; p < kGeoBlock; ++p) {
-          const double ddx = st_dsub(st_dmul(kdx[p], J.d), ax[p]);
-          const double ddy = st_dsub(st_dmul(kdy[p], J.d), ay[p]);
-          const double dz2 = __ldg(&P.PDZ2[tb + (h4 + p) * 32]);
-          const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dz2);
-          const bool hit = ((boxmask >> (h4 + p)) & 1u) && dist <= J.r2;
-          hitmask |= (unsigned)hit << (h4 + p);
-          kxv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdx[p], kMagic));
-          kyv[h4 + p] = (uint32_t)__double2loint(st_dadd(kdy[p], kMagic));
-        }
-      }
-      }
-      hits += __popc(hitmask);
-      inbox += __popc(boxmask);
-      // runs of equal keys inside the lane's consecutive deposits are summed in registers
-      uint64_t rkey = kEmptyKey, rlo = 0, rhi = 0;
-      bool rflag = false;
-#pragma unroll
-      for (int p = 0; p < kDepPerLane; ++p) {
-        if (hitmask & (1u << p)) {
-          const int64_t idx = tb + p * 32;
-          const uint64_t lo = __ldg(&P.PVLO[idx]);
-          const uint64_t hi = __ldg(&P.PVHI[idx]);
-          const uint64_t kzw = __ldg(&P.PKEY[idx]);
-          // (the FP32 form converts a lattice index like the reference's llrint: sign-extended)
-          const uint64_t key =
-              (F32 ? (uint64_t)(int64_t)(int32_t)kxv[p] + (uint64_t)(int64_t)(int32_t)kyv[p] * J.N
-                   : (uint64_t)kxv[p] + (uint64_t)kyv[p] * J.N) + (kzw & ~kBoundaryBit);
-          const bool bflag = (kzw & kBoundaryBit) != 0;
-          if (key == rkey) {
-            add128(rlo, rhi, lo, hi);
-            rflag |= bflag;
-          } else {
-            if (rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
-            rkey = key; rlo = lo; rhi = hi; rflag = bflag;
+        // the lanes' last runs: segmented sum over consecutive lanes with the same key, so a
+        // sphere spanning several lanes costs one shared-memory update
+        {
+          const uint64_t kprev = __shfl_up_sync(0xffffffffu, rkey, 1);
+          const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
+          bool head = lane == 0 || kprev != rkey;
+          const bool tail = lane == 31 || knext != rkey;
+          const bool any_run = __any_sync(0xffffffffu, !head && rkey != kEmptyKey);
+  #pragma unroll
+          for (int o = 1; any_run && o < 32; o <<= 1) {
+            const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
+            const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
+            const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
+            const bool oflag = __shfl_up_sync(0xffffffffu, rflag, o);
+            if (lane >= o && !head) {
+              add128(rlo, rhi, olo, ohi);
+              rflag |= oflag;
+              head = ohead;
+            }
           }
+          if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
         }
-      }
-      // the lanes' last runs: segmented sum over consecutive lanes with the same key, so a
-      // sphere spanning several lanes costs one shared-memory update
-      {
-        const uint64_t kprev = __shfl_up_sync(0xffffffffu, rkey, 1);
-        const uint64_t knext = __shfl_down_sync(0xffffffffu, rkey, 1);
-        bool head = lane == 0 || kprev != rkey;
-        const bool tail = lane == 31 || knext != rkey;
-        const bool any_run = __any_sync(0xffffffffu, !head && rkey != kEmptyKey);
-#pragma unroll
-        for (int o = 1; any_run && o < 32; o <<= 1) {
-          const uint64_t olo = __shfl_up_sync(0xffffffffu, rlo, o);
-          const uint64_t ohi = __shfl_up_sync(0xffffffffu, rhi, o);
-          const bool ohead = __shfl_up_sync(0xffffffffu, head, o);
-          const bool oflag = __shfl_up_sync(0xffffffffu, rflag, o);
-          if (lane >= o && !head) {
-            add128(rlo, rhi, olo, ohi);
-            rflag |= oflag;
-            head = ohead;
-          }
-        }
-        if (tail && rkey != kEmptyKey) sphere_add<CAP>(T, &cs, P, G, rkey, rlo, rhi, rflag, slot);
       }
     }
     if (J.flagged) {
@@ -990,7 +994,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       // the table and its boundary bits are clear again once every thread is past this point
       sent = __syncthreads_or(sent);
       if (sent && tid == 0) cs.spilled = 1;
-    } else if (window_checks && wt0 + kWarps < wt_end) {
+    } else if (window_checks && wt0 + kWarps * kWinTiles < wt_end) {
       __syncthreads();
       if (cs.tc[0] > P.flush_threshold) {
         if (log_mode) flush_to_log<CAP, THREADS>(T, cs.tc[0], &cs, P, G);
@@ -1089,7 +1093,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     // Segments: a private item walks its oversamples (all windows each) with one pool table; a
     // helper claims window chunks of its shared unit until none is left.
     const bool shared = W.unit >= 0;
-    const int64_t wpc = (int64_t)P.chunk_windows * kFusedWarps;  // warp tiles per chunk
+    const int64_t wpc = (int64_t)P.chunk_windows * kFusedWarps * kWinTiles;  // warp tiles per chunk
     const int64_t n_chunks = (F.n_wt + wpc - 1) / wpc;
     int private_table = -1;
     if (!shared) {
