@@ -80,6 +80,7 @@ struct JobAux {
   unsigned long long spheres;  // (oversample, sphere) pairs with at least one hit
   unsigned long long binned;   // of those, the ones that landed inside the histogram range
   unsigned long long inbox;    // deposit*oversamples inside the voxel after the shift
+  unsigned long long cells;    // occupied cells of the boundary-flag hash (windowed jobs)
 };
 constexpr int kAuxNonzero = 1;
 constexpr int kAuxNonfinite = 2;
@@ -213,6 +214,7 @@ constexpr int kPrepSlotsPerBlock = 1024;                // source deposits per p
 constexpr int kFusedWarps = 32;                       // warps of the fused kernel's CTA
 constexpr int kCtaTile = kFusedWarps * kWarpTile;    // kept deposits of one warp tile per warp
 constexpr int kWinTiles = 2;                          // warp tiles per warp in a window
+constexpr int kCoarseTiles = 4;                       // ... in a coarse window (dense spheres)
 constexpr int kWindow = kWinTiles * kCtaTile;         // kept deposits per window (8192)
 constexpr int kCellBits = 21;                         // bits per axis of a cell key
 

@@ -64,6 +64,14 @@ __device__ __forceinline__ int find_job(const int64_t* blk_prefix, int n_jobs, i
   return lo;
 }
 
+// A windowed job whose kept deposits share cells (fewer than half as many occupied cells as
+// deposits: several hits per sphere) runs with coarse windows of kCoarseTiles warp tiles per
+// warp; others with kWinTiles. Its cells record windows of kWindow deposits, a coarse window is
+// two of them.
+__device__ __forceinline__ bool coarse_windows(const JobAux& A) {
+  return A.windowed && 2 * (long long)A.cells < A.kept;
+}
+
 __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y, double z) {
   const double z1 = st_dadd(z, J.zsh);
   return fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
@@ -88,35 +96,41 @@ __device__ __forceinline__ uint64_t cell_key(const CellCoord& c, int dx, int dy,
          (uint64_t)(c.x + dx);
 }
 
-__device__ __forceinline__ void cell_insert(const PrepareParams& p, const JobDev& J,
+// Records window `win` in the cell `key`; true when this call created the cell.
+__device__ __forceinline__ bool cell_insert(const PrepareParams& p, const JobDev& J,
                                             uint64_t key, uint32_t win) {
   const uint32_t mask = J.cell_cap - 1;
   uint32_t h = slot_hash(key, mask);
   for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
     CellSlot* slot = p.cells + J.cell_off + h;
     const uint64_t k = __ldcg(&slot->key);
-    bool mine = k == key;
+    bool mine = k == key, created = false;
     if (!mine && k == kEmptyKey) {
       const uint64_t old = atomicCAS(&slot->key, kEmptyKey, key);
-      mine = old == kEmptyKey || old == key;
+      created = old == kEmptyKey;
+      mine = created || old == key;
     }
     if (mine) {
       atomicMin(&slot->wmin, win);
       atomicMin(&slot->nwmax, ~win);
-      return;
+      return created;
     }
     h = (h + 1) & mask;
   }
+  return false;
 }
 
-// True when the cell holds a deposit of a window other than `win`.
+// True when the cell holds a deposit of a window other than `win`; windows are compared after
+// a right shift by `shift` (1: coarse windows of two recorded windows each).
 __device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDev& J,
-                                             uint64_t key, uint32_t win) {
+                                             uint64_t key, uint32_t win, int shift) {
   const uint32_t mask = J.cell_cap - 1;
   uint32_t h = slot_hash(key, mask);
   for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
     const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p.cells + J.cell_off + h));
-    if (v.x == key) return (uint32_t)v.y != win || ~(uint32_t)(v.y >> 32) != win;
+    if (v.x == key)
+      return ((uint32_t)v.y >> shift) != (win >> shift) ||
+             (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
     if (v.x == kEmptyKey) return false;
     h = (h + 1) & mask;
   }
@@ -220,6 +234,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
   int64_t run = p.blk_offset[b];  // kept index of the next kept deposit of this block
   const JobAux A = p.aux[j];
   const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
+  unsigned created_cells = 0;  // cells this thread created (windowed jobs)
   for (int r = 0; r < kPrepSlotsPerBlock / kPrepThreads; ++r) {
     const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
     bool keep = false;
@@ -263,11 +278,17 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (A.windowed) {
         p.PZ[dst] = z1;
-        cell_insert(p, J, cell_key(cell_of(x, y, z1, J.cell_size), 0, 0, 0), (uint32_t)(k / kWindow));
+        created_cells +=
+            cell_insert(p, J, cell_key(cell_of(x, y, z1, J.cell_size), 0, 0, 0), (uint32_t)(k / kWindow));
       }
     }
     run += total;
     __syncthreads();
+  }
+  if (A.windowed) {  // occupied cells, one addition per warp (the window size depends on them)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) created_cells += __shfl_xor_sync(0xffffffffu, created_cells, o);
+    if (lane == 0 && created_cells) atomicAdd(&p.aux[j].cells, (unsigned long long)created_cells);
   }
 }
 
@@ -303,7 +324,9 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = find_job(p.blk_prefix, p.n_jobs, b);
   const JobDev J = p.jobs[j];
-  if (!p.aux[j].windowed) return;
+  const JobAux A = p.aux[j];
+  if (!A.windowed) return;
+  const int shift = coarse_windows(A) ? 1 : 0;
   const int64_t k0 = p.blk_offset[b];
   const int cnt = p.blk_count[b];
   for (int q = threadIdx.x; q < cnt; q += kPrepThreads) {
@@ -325,7 +348,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     const CellCoord cc = cell_of(x, y, z, J.cell_size);
     bool boundary = false;
     for (int c = 0; c < 27 && !boundary; ++c)
-      boundary = cell_foreign(p, J, cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win);
+      boundary = cell_foreign(p, J, cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win, shift);
     if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
 }
@@ -799,8 +822,17 @@ __device__ __forceinline__ void log_reduce(const SmemTable<CAP>& T, CtaState& cs
 struct FusedJob {
   JobDev J;
   int E0;
+  int win_tiles;    // warp tiles per warp in a window: kWinTiles, or kCoarseTiles
   int64_t n_wt;     // warp tiles of kept deposits
 };
+
+// Warp tiles of a shared unit's chunk: chunk_windows windows of kWinTiles tiles per warp,
+// rounded up to whole coarse windows, so that no window is ever split between two chunks.
+__host__ __device__ __forceinline__ int64_t chunk_tiles(int chunk_windows) {
+  constexpr int64_t kCoarse = (int64_t)kFusedWarps * kCoarseTiles;
+  const int64_t t = (int64_t)chunk_windows * kFusedWarps * kWinTiles;
+  return (t + kCoarse - 1) / kCoarse * kCoarse;
+}
 
 // Superimposes oversample `os` of a job over warp tiles [wt_begin, wt_end) (whole windows):
 // shift, box test, lattice test, key, exact run / warp / shared-memory reduction. For flagged jobs
@@ -832,11 +864,12 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   const bool window_checks = CAP < 2 * kCtaTile && !J.flagged &&
                              (uint64_t)J.N * J.N2 > (uint64_t)P.flush_threshold;
   int wi = 0;  // window index within this call
-  for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps * kWinTiles) {
+  const int wtiles = F.win_tiles;
+  for (int64_t wt0 = wt_begin; wt0 < wt_end; wt0 += kWarps * wtiles) {
     const int slot = J.flagged ? wi % 3 : 0;
-    // a window is kWinTiles warp tiles per warp
+    // a window is wtiles warp tiles per warp
 #pragma unroll 1
-    for (int tt = 0; tt < kWinTiles; ++tt) {
+    for (int tt = 0; tt < wtiles; ++tt) {
       const int64_t w = wt0 + tt * kWarps + warp;
       if (w < wt_end) {
         const int64_t tb = J.prep_off + w * kWarpTile + lane;
@@ -994,7 +1027,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
       // the table and its boundary bits are clear again once every thread is past this point
       sent = __syncthreads_or(sent);
       if (sent && tid == 0) cs.spilled = 1;
-    } else if (window_checks && wt0 + kWarps * kWinTiles < wt_end) {
+    } else if (window_checks && wt0 + kWarps * wtiles < wt_end) {
       __syncthreads();
       if (cs.tc[0] > P.flush_threshold) {
         if (log_mode) flush_to_log<CAP, THREADS>(T, cs.tc[0], &cs, P, G);
@@ -1058,6 +1091,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     FusedJob F;
     F.J = P.jobs[W.job];
     F.J.flagged = A.windowed;  // window flags were computed only for these jobs
+    F.win_tiles = coarse_windows(A) ? kCoarseTiles : kWinTiles;
     F.E0 = choose_grid_exponent(A.e_min, A.e_max, F.J.n, A.flags & kAuxNonzero);
     F.n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
     const HistDev H = P.hists[F.J.hist];
@@ -1093,7 +1127,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     // Segments: a private item walks its oversamples (all windows each) with one pool table; a
     // helper claims window chunks of its shared unit until none is left.
     const bool shared = W.unit >= 0;
-    const int64_t wpc = (int64_t)P.chunk_windows * kFusedWarps * kWinTiles;  // warp tiles per chunk
+    const int64_t wpc = chunk_tiles(P.chunk_windows);  // warp tiles per chunk
     const int64_t n_chunks = (F.n_wt + wpc - 1) / wpc;
     int private_table = -1;
     if (!shared) {
@@ -1257,7 +1291,7 @@ __global__ void k_plan_size(PlanParams q) {
   pl.unit_base = -1;
   pl.blk_os = 1;
   if (kept > 0 && nos > 0 && !(q.aux[j].flags & kAuxNonfinite)) {
-    const long long chunk = (long long)q.chunk_windows * kWindow;
+    const long long chunk = chunk_tiles(q.chunk_windows) * kWarpTile;
     const long long share =
         q.share_divisor > 0 ? (long long)(*q.total_units / ((unsigned long long)q.share_divisor * q.grid)) : 0;
     if (q.share_divisor > 0 && kept > (long long)q.min_chunks * chunk && kept > share) {
@@ -1335,6 +1369,7 @@ __global__ void k_reset_aux(JobAux* aux, int n) {
   a.spheres = 0;
   a.binned = 0;
   a.inbox = 0;
+  a.cells = 0;
   aux[j] = a;
 }
 
