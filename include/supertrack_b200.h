@@ -160,7 +160,7 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   flag_min_kept      a multi-window job on a fine lattice (more than 8192 deposits, at least 4
  *                      oversamples, 128 or more spheres along an axis) gets window boundary flags
  *                      when more than this many of its deposits are kept; with fewer, its
- *                      spheres fit the shared-memory table without them      (default 8192)
+ *                      spheres fit the shared-memory table without them      (default 16384)
  *   precision          64 = the reference's FP64 arithmetic; 32 = FP32 geometry variant: x, y,
  *                      shifts, the x/y box test, x/y lattice index and sphere distance in float
  *                      (z, keys and energies as in FP64). No reference counterpart: the

@@ -199,7 +199,7 @@ struct st_ctx {
   int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
   int min_chunks = 4;         // ... and kept > min_chunks chunks
   int precision = 64;         // 32: FP32 geometry variant (x/y geometry in float)
-  int64_t flag_min_kept = 8192;   // window flags only for jobs with more kept deposits
+  int64_t flag_min_kept = 16384;  // window flags only for jobs with more kept deposits
 
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
