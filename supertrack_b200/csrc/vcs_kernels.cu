@@ -143,9 +143,11 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
   const JobDev J = p.jobs[j];
   const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
   int emin = INT_MAX, emax = INT_MIN, flags = 0, kept = 0;
+  // a guard rather than a break, so that the loads of all rounds can be in flight together
+#pragma unroll
   for (int s = threadIdx.x; s < kPrepSlotsPerBlock; s += kPrepThreads) {
     const int64_t i = i0 + s;
-    if (i >= J.n) break;
+    if (i >= J.n) continue;
     kept += keep_deposit(J, J.x[i], J.y[i], J.z[i]) ? 1 : 0;
     const double v = __ddiv_rn(J.edep[i], J.denom);
     if (!isfinite(v)) {
