@@ -167,7 +167,7 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *                      reference's readme asks for a float form (readme.md:29). Results are
  *                      not bound to the reference's                           (default 64)
  *   table_slots        shared-memory sphere table: 0 = 8192 slots when every histogram has at
- *                      most 900 bins, else 4096; 4096 = always 4096          (default 0)
+ *                      most 600 bins, else 4096; 4096 = always 4096          (default 0)
  *   pipeline_bytes     runs with host-resident tracks upload them in groups on a second stream
  *                      while earlier groups compute; groups hold about this many bytes of
  *                      track data (the first and last about a quarter); 0 = one upload, then

@@ -520,7 +520,8 @@ struct BinContext {
   unsigned long long* gcounts;
   double* gyfy;
   unsigned int* hcount;   // null: accumulate straight into HBM
-  double* hyfy;
+  unsigned long long* hylo;  // y*f(y) per bin: 128-bit sum on the bin's grid (see bin_sphere)
+  unsigned long long* hyhi;
   int copies;             // shared-memory copies of the histogram, used by warp % copies
   int nbins;
   int mode;               // 0: linear candidate, 1: log2 candidate
@@ -564,7 +565,18 @@ __device__ __forceinline__ void bin_sphere(const BinContext& B, const FusedParam
       // warps spread over the copies, so that fewer of them contend for a bin's 64-bit add
       const int c = B.copies > 1 ? (int)((threadIdx.x >> 5) % (unsigned)B.copies) * B.nbins : 0;
       atomicAdd(&B.hcount[c + b], 1u);
-      atomicAdd(&B.hyfy[c + b], y);
+      // y >= edge_b > 0 is a whole multiple of ulp(edge_b): its sum is kept exactly as a 128-bit
+      // integer on that grid, with integer atomics (a double atomic add is a retry loop under
+      // contention). A bin whose lower edge is not a positive normal number keeps a double sum
+      // in the low word instead.
+      const uint64_t eb = (uint64_t)__double_as_longlong(B.edges[b]);
+      if ((int64_t)eb > 0 && (eb >> 52) != 0) {
+        uint64_t lo, hi;
+        to_fixed(y, (int)(eb >> 52) - 1075, &lo, &hi);
+        acc_add(&B.hylo[c + b], &B.hyhi[c + b], lo, hi);
+      } else {
+        atomicAdd(reinterpret_cast<double*>(&B.hylo[c + b]), y);
+      }
     } else {
       atomicAdd(&B.gcounts[b], 1ull);
       atomicAdd(&B.gyfy[b], y);
@@ -1060,15 +1072,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
 
   const int HB = P.smem_hist_bins;
   const SmemTable<CAP> T;
-  double* hyfy = SmemTable<CAP>::hist();
-  double* sedges = hyfy + HB;                                   // HB + 1 edges
+  unsigned long long* hylo = reinterpret_cast<unsigned long long*>(SmemTable<CAP>::hist());
+  unsigned long long* hyhi = hylo + HB;
+  double* sedges = reinterpret_cast<double*>(hyhi + HB);         // HB + 1 edges
   unsigned int* hcount = reinterpret_cast<unsigned int*>(sedges + HB + 1);
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
 
   for (int i = tid; i < CAP; i += THREADS) { T.keys()[i] = kEmptyKey; T.lo()[i] = 0; T.hi()[i] = 0; }
-  for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hyfy[i] = 0.0; }
+  for (int i = tid; i < HB; i += THREADS) { hcount[i] = 0; hylo[i] = 0; hyhi[i] = 0; }
   for (int i = tid; i < CAP / 32; i += THREADS) T.flags()[i] = 0;
   if (tid == 0) {
     for (int k = 0; k < 3; ++k) { cs.tc[k] = 0; cs.ovf[k] = 0; }
@@ -1117,7 +1130,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
       sB.E0 = F.E0;
       sB.job = W.job;
       sB.hcount = smem_hist ? hcount : nullptr;
-      sB.hyfy = smem_hist ? hyfy : nullptr;
+      sB.hylo = smem_hist ? hylo : nullptr;
+      sB.hyhi = smem_hist ? hyhi : nullptr;
       sB.copies = smem_hist ? min(kHistCopies, HB / H.nbins) : 1;
     }
     __syncthreads();
@@ -1227,18 +1241,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     if (smem_hist) {
       const int copies = B.copies;
       for (int b = tid; b < H.nbins; b += THREADS) {
+        const uint64_t eb = (uint64_t)__double_as_longlong(sedges[b]);
+        const bool exact = (int64_t)eb > 0 && (eb >> 52) != 0;  // as in bin_sphere
         unsigned cnt = 0;
+        uint64_t lo = 0, hi = 0;
         double ys = 0.0;
         for (int c = 0; c < copies; ++c) {
           const int i = c * H.nbins + b;
           cnt += hcount[i];
-          ys += hyfy[i];
+          if (exact) add128(lo, hi, hylo[i], hyhi[i]);
+          else ys += __longlong_as_double((long long)hylo[i]);
           hcount[i] = 0;
-          hyfy[i] = 0.0;
+          hylo[i] = 0;
+          hyhi[i] = 0;
         }
         if (cnt) {
           atomicAdd(&H.counts[b], (unsigned long long)cnt);
-          atomicAdd(&H.yfy[b], ys);
+          atomicAdd(&H.yfy[b], exact ? from_fixed(lo, hi, (int)(eb >> 52) - 1075) : ys);
         }
       }
     }
@@ -1424,11 +1443,11 @@ constexpr int kFusedThreads = 1024;
 // Two shapes of the fused kernel: a 4096-slot sphere table with room for histograms of up to
 // 4096 bins in shared memory, or an 8192-slot table when every histogram of the batch has at
 // most kSmallHistBins bins.
-constexpr int kSmallHistBins = 900;
+constexpr int kSmallHistBins = 600;
 constexpr int kBigHistBins = 4096;
 
 size_t fused_smem_bytes(int cap, int hist_bins) {
-  return (size_t)cap * 26 + (size_t)cap / 8 + (size_t)hist_bins * 20 + 8;
+  return (size_t)cap * 26 + (size_t)cap / 8 + (size_t)hist_bins * 28 + 8;
 }
 
 cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_flagged,
