@@ -127,7 +127,9 @@ __device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDe
   const uint32_t mask = J.cell_cap - 1;
   uint32_t h = slot_hash(key, mask);
   for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
-    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(p.cells + J.cell_off + h));
+    // read-only here (k_prep_write filled the hash): the neighbourhoods of a block's consecutive
+    // deposits overlap, so cached loads serve many probes from L1
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p.cells + J.cell_off + h));
     if (v.x == key)
       return ((uint32_t)v.y >> shift) != (win >> shift) ||
              (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
