@@ -63,9 +63,10 @@ struct JobDev {
   float f_pad;
 };
 
-// Deposits are processed in windows of kWindow consecutive kept deposits (two warp tiles per warp
-// of the fused kernel's CTA). A kept deposit is a boundary deposit when a kept deposit of another window lies
-// within distance d of it; the flag travels in bit 63 of its PKEY word (keys are below 2^63).
+// Deposits of a windowed job are processed in windows of consecutive kept deposits: kWindow (two
+// warp tiles per warp of the fused kernel's CTA), or twice that for jobs with coarse windows. A
+// kept deposit is a boundary deposit when a kept deposit of another window lies within distance d
+// of it; the flag travels in bit 63 of its PKEY word (keys are below 2^63).
 constexpr unsigned long long kBoundaryBit = 1ull << 63;
 
 // Per-job values produced on the device.
