@@ -138,7 +138,7 @@ struct st_ctx {
 
   DevBuf track_arena;
   DevBuf px, py, pdz2, pvlo, pvhi, pkey;
-  DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off;
+  DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off, d_blk_job;
   DevBuf c_cells, pz;               // cell arena and shifted z of flagged jobs
   DevBuf u_next, u_done, u_table, pool;  // shared units and the spill-table pool
   DevBuf d_plan, d_plan_misc;             // planner: per-job plans and scratch counters
@@ -417,6 +417,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   ST_CUDA(ensure(c->d_hists, std::max<size_t>(1, hd.size()) * sizeof(HistDev)), "hist table");
   ST_CUDA(ensure(c->d_blk, (nj + 1) * 8), "prepare blocks");
   ST_CUDA(ensure(c->d_blk_count, (size_t)blk[nj] * 4), "prepare block counts");
+  ST_CUDA(ensure(c->d_blk_job, (size_t)std::max<int64_t>(1, blk[nj]) * 4), "prepare block jobs");
   ST_CUDA(ensure(c->c_cells, (size_t)cells_total * sizeof(st::CellSlot)), "cell arena");
   ST_CUDA(ensure(c->pz, any_flagged ? (size_t)prep_total * 8 : 16), "shifted z");
   ST_CUDA(ensure(c->d_blk_off, (size_t)blk[nj] * 8), "prepare block offsets");
@@ -426,15 +427,21 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     // tables through pinned staging (the previous run's copies from it have completed)
     const size_t o_hists = align256(nj * sizeof(JobDev));
     const size_t o_blk = o_hists + align256(hd.size() * sizeof(HistDev));
-    ST_CUDA(ensure_pinned(c->stage, o_blk + align256((nj + 1) * 8)), "pinned staging");
+    const size_t o_bj = o_blk + align256((nj + 1) * 8);
+    ST_CUDA(ensure_pinned(c->stage, o_bj + align256((size_t)blk[nj] * 4)), "pinned staging");
     char* st_base = (char*)c->stage.p;
     std::memcpy(st_base, jd.data(), nj * sizeof(JobDev));
     if (!hd.empty()) std::memcpy(st_base + o_hists, hd.data(), hd.size() * sizeof(HistDev));
     std::memcpy(st_base + o_blk, blk.data(), (nj + 1) * 8);
+    int32_t* bj = (int32_t*)(st_base + o_bj);  // job of each prepare block
+    for (size_t i = 0; i < nj; ++i)
+      for (int64_t b = blk[i]; b < blk[i + 1]; ++b) bj[b] = (int32_t)i;
     ST_CUDA(cudaMemcpyAsync(c->d_jobs.p, st_base, nj * sizeof(JobDev), cudaMemcpyHostToDevice, c->stream), "upload jobs");
     if (!hd.empty())
       ST_CUDA(cudaMemcpyAsync(c->d_hists.p, st_base + o_hists, hd.size() * sizeof(HistDev), cudaMemcpyHostToDevice, c->stream), "upload hists");
     ST_CUDA(cudaMemcpyAsync(c->d_blk.p, st_base + o_blk, (nj + 1) * 8, cudaMemcpyHostToDevice, c->stream), "upload blocks");
+    if (blk[nj] > 0)
+      ST_CUDA(cudaMemcpyAsync(c->d_blk_job.p, st_base + o_bj, (size_t)blk[nj] * 4, cudaMemcpyHostToDevice, c->stream), "upload block jobs");
   }
 
   // spill tables: one per resident CTA, able to hold every distinct sphere of the largest job;
@@ -474,6 +481,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.n_jobs = (int32_t)nj;
   pp.blk_base = 0;
   pp.blk_prefix = (const int64_t*)c->d_blk.p;
+  pp.blk_job = (const int32_t*)c->d_blk_job.p;
+  pp.job_base = 0;
   pp.blk_count = (int32_t*)c->d_blk_count.p;
   pp.blk_offset = (int64_t*)c->d_blk_off.p;
   pp.cells = (st::CellSlot*)c->c_cells.p;
@@ -628,6 +637,7 @@ st_status enqueue_groups(st_ctx* c, const st::FusedParams& fp, size_t first,
     pp.aux += j0;
     pp.n_jobs = (int32_t)(j1 - j0);
     pp.blk_prefix += j0;
+    pp.job_base = (int32_t)j0;
     pp.blk_base = c->cache_blk[j0];
     bool flagged = false;
     for (size_t j = j0; j < j1; ++j) flagged |= c->cache_flagged[j] != 0;
@@ -1015,7 +1025,7 @@ st_status st_ctx_destroy(st_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pvlo, &c->pvhi, &c->pkey,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
-                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->c_cells,
+                    &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->d_blk_job, &c->c_cells,
                     &c->pz, &c->u_next, &c->u_done, &c->u_table,
                     &c->pool, &c->d_plan, &c->d_plan_misc, &c->g_keys, &c->g_lo, &c->g_hi,
                     &c->g_used, &c->g_count, &c->ex_buf, &c->ex_count, &c->h_counts,

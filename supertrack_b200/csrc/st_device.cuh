@@ -166,6 +166,9 @@ struct PrepareParams {
   int64_t blk_base;           // prepare block of blockIdx.x 0 (jobs and blk_prefix may start
                               // at a later job of the batch; block indices stay batch-wide)
   const int64_t* blk_prefix;  // n_jobs+1 prefix sums of prepare blocks per job
+  const int32_t* blk_job;     // batch-wide job index of each prepare block (null: searched in
+                              // blk_prefix)
+  int32_t job_base;           // batch-wide index of jobs[0]
   int32_t* blk_count;         // kept deposits per prepare block
   int64_t* blk_offset;        // first kept index of each prepare block inside its job
   CellSlot* cells;            // cell arena (flagged jobs)

@@ -64,6 +64,12 @@ __device__ __forceinline__ int find_job(const int64_t* blk_prefix, int n_jobs, i
   return lo;
 }
 
+// The job of prepare block b: one load from the block table, which saves the short prepare
+// blocks a dozen dependent loads of the binary search before their first track load.
+__device__ __forceinline__ int prep_job(const PrepareParams& p, int64_t b) {
+  return p.blk_job ? __ldg(&p.blk_job[b]) - p.job_base : find_job(p.blk_prefix, p.n_jobs, b);
+}
+
 // A windowed job whose kept deposits share cells (fewer than half as many occupied cells as
 // deposits: several hits per sphere) runs with coarse windows of kCoarseTiles warp tiles per
 // warp; others with kWinTiles. Its cells record windows of kWindow deposits, a coarse window is
@@ -141,7 +147,7 @@ __device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDe
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
-  const int j = find_job(p.blk_prefix, p.n_jobs, b);
+  const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
   const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
   int emin = INT_MAX, emax = INT_MIN, flags = 0, kept = 0;
@@ -229,65 +235,79 @@ __global__ void __launch_bounds__(1024) k_prep_scan(PrepareParams p) {
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
-  const int j = find_job(p.blk_prefix, p.n_jobs, b);
+  const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
   const int64_t i0 = (b - p.blk_prefix[j]) * (int64_t)kPrepSlotsPerBlock;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarpsPerBlock = kPrepThreads / 32;
-  __shared__ int s_warp[kWarpsPerBlock];
+  constexpr int kRounds = kPrepSlotsPerBlock / kPrepThreads;
+  __shared__ int s_warp[kRounds][kWarpsPerBlock];
   int64_t run = p.blk_offset[b];  // kept index of the next kept deposit of this block
   const JobAux A = p.aux[j];
   const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
   unsigned created_cells = 0;  // cells this thread created (windowed jobs)
-  for (int r = 0; r < kPrepSlotsPerBlock / kPrepThreads; ++r) {
+  // the loads of all rounds are issued before the block's one barrier, so each thread has all
+  // of its source deposits in flight at once
+  double x[kRounds], y[kRounds], z1[kRounds], e[kRounds];
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
     const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
-    bool keep = false;
-    double x = 0, y = 0, z1 = 0;
+    x[r] = 0; y[r] = 0; z1[r] = 0;
     if (i < J.n) {
-      x = J.x[i];
-      y = J.y[i];
-      z1 = st_dadd(J.z[i], J.zsh);
-      keep = fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
+      x[r] = J.x[i];
+      y[r] = J.y[i];
+      z1[r] = J.z[i];
     }
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) s_warp[warp] = __popc(m);
-    __syncthreads();
+  }
+  unsigned keep = 0, m[kRounds];
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
+    const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
+    z1[r] = st_dadd(z1[r], J.zsh);
+    const bool k = i < J.n && fabs(z1[r]) < J.HL && fabs(x[r]) < J.xy_keep && fabs(y[r]) < J.xy_keep;
+    keep |= k ? 1u << r : 0u;
+    m[r] = __ballot_sync(0xffffffffu, k);
+    if (lane == 0) s_warp[r][warp] = __popc(m[r]);
+    e[r] = k ? J.edep[i] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kRounds; ++r) {
     int before = 0, total = 0;
 #pragma unroll
     for (int w = 0; w < kWarpsPerBlock; ++w) {
-      const int c = s_warp[w];
+      const int c = s_warp[r][w];
       before += (w < warp) ? c : 0;
       total += c;
     }
-    if (keep) {
-      const int64_t k = run + before + __popc(m & ((1u << lane) - 1u));
-      const double az = st_dsub(z1, J.gSO);
+    if (keep & (1u << r)) {
+      const int64_t k = run + before + __popc(m[r] & ((1u << lane) - 1u));
+      const double az = st_dsub(z1[r], J.gSO);
       const double kd = rint(__ddiv_rn(az, J.d));
       const double dz = st_dsub(st_dmul(kd, J.d), az);
       const int64_t w = k / kWarpTile;
       const int rem = (int)(k - w * kWarpTile);
       const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
       if (p.fp32) {
-        reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__double2float_rn(x), __double2float_rn(y));
+        reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__double2float_rn(x[r]), __double2float_rn(y[r]));
         reinterpret_cast<float*>(p.PDZ2)[dst] = __double2float_rn(st_dmul(dz, dz));
       } else {
-        p.PX[dst] = x;
-        p.PY[dst] = y;
+        p.PX[dst] = x[r];
+        p.PY[dst] = y[r];
         p.PDZ2[dst] = st_dmul(dz, dz);
       }
       uint64_t lo, hi;
-      to_fixed(__ddiv_rn(J.edep[i], J.denom), E0, &lo, &hi);
+      to_fixed(__ddiv_rn(e[r], J.denom), E0, &lo, &hi);
       p.PVLO[dst] = lo;
       p.PVHI[dst] = hi;
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (A.windowed) {
-        p.PZ[dst] = z1;
-        created_cells +=
-            cell_insert(p, J, cell_key(cell_of(x, y, z1, J.cell_size), 0, 0, 0), (uint32_t)(k / kWindow));
+        p.PZ[dst] = z1[r];
+        created_cells += cell_insert(p, J, cell_key(cell_of(x[r], y[r], z1[r], J.cell_size), 0, 0, 0),
+                                     (uint32_t)(k / kWindow));
       }
     }
     run += total;
-    __syncthreads();
   }
   if (A.windowed) {  // occupied cells, one addition per warp (the window size depends on them)
 #pragma unroll
@@ -326,7 +346,7 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
 // so the fused kernel can bin it as soon as the window is done.
 __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
-  const int j = find_job(p.blk_prefix, p.n_jobs, b);
+  const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
   const JobAux A = p.aux[j];
   if (!A.windowed) return;
