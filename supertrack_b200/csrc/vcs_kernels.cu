@@ -126,23 +126,54 @@ __device__ __forceinline__ bool cell_insert(const PrepareParams& p, const JobDev
   return false;
 }
 
-// True when the cell holds a deposit of a window other than `win`; windows are compared after
-// a right shift by `shift` (1: coarse windows of two recorded windows each).
-__device__ __forceinline__ bool cell_foreign(const PrepareParams& p, const JobDev& J,
-                                             uint64_t key, uint32_t win, int shift) {
+// True when the cell slot v holds a deposit of a window other than `win`; windows are compared
+// after a right shift by `shift` (1: coarse windows of two recorded windows each).
+__device__ __forceinline__ bool slot_foreign(const ulonglong2& v, uint32_t win, int shift) {
+  return ((uint32_t)v.y >> shift) != (win >> shift) ||
+         (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
+}
+
+// True when one of the neighbour cells c0 .. c0 + kFlagBatch - 1 (of the 27 around cc) holds a
+// deposit of another window. Their first hash slots are loaded together, so a lane has three
+// L2 round trips in flight instead of one; a cell whose first slot holds another key continues
+// probing alone. The hash is read-only here (k_prep_write filled it), and the neighbourhoods of
+// a block's deposits overlap, so cached loads serve many probes from L1.
+constexpr int kFlagBatch = 3;
+__device__ __forceinline__ bool cells_foreign(const PrepareParams& p, const JobDev& J,
+                                              const CellCoord& cc, int c0, uint32_t win, int shift) {
   const uint32_t mask = J.cell_cap - 1;
-  uint32_t h = slot_hash(key, mask);
-  for (uint32_t probe = 0; probe < J.cell_cap; ++probe) {
-    // read-only here (k_prep_write filled the hash): the neighbourhoods of a block's consecutive
-    // deposits overlap, so cached loads serve many probes from L1
-    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p.cells + J.cell_off + h));
-    if (v.x == key)
-      return ((uint32_t)v.y >> shift) != (win >> shift) ||
-             (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
-    if (v.x == kEmptyKey) return false;
-    h = (h + 1) & mask;
+  const CellSlot* base = p.cells + J.cell_off;
+  ulonglong2 v[kFlagBatch];
+  uint32_t h[kFlagBatch];
+#pragma unroll
+  for (int t = 0; t < kFlagBatch; ++t) {
+    const int c = c0 + t;
+    h[t] = slot_hash(cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), mask);
+    v[t] = __ldg(reinterpret_cast<const ulonglong2*>(base + h[t]));
   }
-  return true;
+  bool foreign = false;
+#pragma unroll
+  for (int t = 0; t < kFlagBatch; ++t) {
+    const int c = c0 + t;
+    const uint64_t key = cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1);
+    if (v[t].x == key) {
+      foreign |= slot_foreign(v[t], win, shift);
+    } else if (v[t].x != kEmptyKey) {
+      uint32_t hh = h[t];
+#pragma unroll 1
+      for (uint32_t probe = 1; probe < J.cell_cap; ++probe) {
+        hh = (hh + 1) & mask;
+        const ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(base + hh));
+        if (w.x == key) {
+          foreign |= slot_foreign(w, win, shift);
+          break;
+        }
+        if (w.x == kEmptyKey) break;
+        if (probe == J.cell_cap - 1) foreign = true;  // a full table: conservative
+      }
+    }
+  }
+  return foreign;
 }
 
 __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
@@ -371,8 +402,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     const uint32_t win = (uint32_t)(k / kWindow);
     const CellCoord cc = cell_of(x, y, z, J.cell_size);
     bool boundary = false;
-    for (int c = 0; c < 27 && !boundary; ++c)
-      boundary = cell_foreign(p, J, cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), win, shift);
+    for (int c0 = 0; c0 < 27 && !boundary; c0 += kFlagBatch)
+      boundary = cells_foreign(p, J, cc, c0, win, shift);
     if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
 }
