@@ -205,21 +205,35 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
     flags |= __shfl_xor_sync(0xffffffffu, flags, o);
     kept += __shfl_xor_sync(0xffffffffu, kept, o);
   }
-  __shared__ int s_kept;
-  if (threadIdx.x == 0) s_kept = 0;
+  // the block's warps meet in shared memory; one thread updates the job's record, whose
+  // address every block of the job shares
+  __shared__ int s_kept, s_flags, s_emin, s_emax;
+  if (threadIdx.x == 0) {
+    s_kept = 0;
+    s_flags = 0;
+    s_emin = INT_MAX;
+    s_emax = INT_MIN;
+  }
   __syncthreads();
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&s_kept, kept);
     if (flags) {
-      atomicOr(&p.aux[j].flags, flags);
-      if (flags & kAuxNonzero) {
-        atomicMin(&p.aux[j].e_min, emin);
-        atomicMax(&p.aux[j].e_max, emax);
-      }
+      atomicOr(&s_flags, flags);
+      atomicMin(&s_emin, emin);
+      atomicMax(&s_emax, emax);
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) p.blk_count[b] = s_kept;
+  if (threadIdx.x == 0) {
+    p.blk_count[b] = s_kept;
+    if (s_flags) {
+      atomicOr(&p.aux[j].flags, s_flags);
+      if (s_flags & kAuxNonzero) {
+        atomicMin(&p.aux[j].e_min, s_emin);
+        atomicMax(&p.aux[j].e_max, s_emax);
+      }
+    }
+  }
 }
 
 // One CTA per job: exclusive scan of the job's block counts.
@@ -340,10 +354,15 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
     }
     run += total;
   }
-  if (A.windowed) {  // occupied cells, one addition per warp (the window size depends on them)
+  if (A.windowed) {  // occupied cells, one addition per block (the window size depends on them)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) created_cells += __shfl_xor_sync(0xffffffffu, created_cells, o);
-    if (lane == 0 && created_cells) atomicAdd(&p.aux[j].cells, (unsigned long long)created_cells);
+    __shared__ unsigned s_cells;
+    if (threadIdx.x == 0) s_cells = 0;
+    __syncthreads();
+    if (lane == 0 && created_cells) atomicAdd(&s_cells, created_cells);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cells) atomicAdd(&p.aux[j].cells, (unsigned long long)s_cells);
   }
 }
 
