@@ -13,7 +13,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     # Build the product library and the oracle in-tree when they are missing (they are built
-    # artefacts: on a GPU box they arrive prebuilt with the repository snapshot).
+    # artefacts: a prebuilt working tree already holds them).
     lib = os.path.join(ROOT, "supertrack_b200", "libsupertrack_b200.so")
     if not os.path.exists(lib):
         subprocess.run(["make", "-C", os.path.join(ROOT, "supertrack_b200"), "-j8"], check=True)
