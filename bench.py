@@ -53,6 +53,29 @@ BYTES_TRACK = 32
 BYTES_PREP = 36
 
 
+def profile_figures(config: int, units: float):
+    """Figures of the committed k_fused ncu capture, for the bench line: DRAM traffic scaled to
+    `units` deposit*oversamples (bytes per unit x units), and the shared-memory roofline term
+    (wavefronts as a fraction of their peak). (None, None) when no capture of this workload
+    exists."""
+    prof = os.path.join(ROOT, "profiles", "fused_traffic.json")
+    try:
+        p = json.load(open(prof))
+    except (OSError, ValueError):
+        return None, None
+    if p.get("config") != config:
+        return None, None
+    traffic = float(p["bytes_per_unit"]) * units if "bytes_per_unit" in p else None
+    smem = None
+    if "smem_wavefront_frac" in p:
+        smem = {"bound": "smem", "frac": float(p["smem_wavefront_frac"]),
+                "unit": "shared-memory wavefronts / peak",
+                "bank_conflict_share": p.get("smem_bank_conflict_share"),
+                "source": p.get("source"),
+                "note": "measured by ncu on a 256-track batch of the same workload (not live)"}
+    return traffic, smem
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -465,15 +488,7 @@ def ours(args, rank, world):
     nbins_total = ctx.total_bins()
     fused_bytes = BYTES_PREP * w.deposits + 16 * nbins_total
     fp64_ops = FP64_OPS_ALL * units + FP64_OPS_INBOX * inbox
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "fused_traffic.json")
-    if os.path.exists(prof):
-        try:
-            p = json.load(open(prof))
-            if p.get("config") == args.config:
-                traffic = p["bytes_per_unit"] * units
-        except Exception:
-            traffic = None
+    traffic, roofline_smem = profile_figures(args.config, units)
     cpu = run_cpu_baseline(w, args.cpu_seconds, os.cpu_count() or 1)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -498,6 +513,7 @@ def ours(args, rank, world):
                           "frac": fp64_ops / (fused_ms * 1e-3) / fp64_peak,
                           "ops_per_launch": fp64_ops,
                           "peak_source": "measured live (dependent add+mul chains)"},
+        "roofline_smem": roofline_smem,
         "clocks": clocks,
         "e2e": e2e,
         "plain": plain,
