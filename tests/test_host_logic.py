@@ -287,6 +287,45 @@ def test_thread_allocation_file_limits(tmp_path):
     assert sorted({t["thread_id"] for t in tasks}) == list(range(6))
 
 
+def test_track_file_layout(tmp_path):
+    """A track file is the magic STRKv001, the deposit and track counts (u64), the cumulative end
+    index of every track (u64, the reference's "Track index" tree), then float64 x, y, z and edep
+    over all deposits (the "Tracks" tree), little-endian."""
+    rs = np.random.default_rng(5)
+    sizes = [3, 0, 7, 1]                      # an empty track included
+    tracks = [tuple(rs.normal(size=n) for _ in range(4)) for n in sizes]
+    p = tmp_path / "t.strk"
+    st.write_track_file(str(p), tracks)
+    raw = p.read_bytes()
+    nd, nt = (int(v) for v in np.frombuffer(raw[8:24], dtype="<u8"))
+    assert raw[:8] == b"STRKv001" and nd == sum(sizes) and nt == len(sizes)
+    assert len(raw) == 24 + 8 * nt + 32 * nd
+    index = np.frombuffer(raw[24:24 + 8 * nt], dtype="<u8")
+    assert index.tolist() == np.cumsum(sizes).tolist()
+    soa = np.frombuffer(raw[24 + 8 * nt:], dtype="<f8").reshape(4, nd)
+    for a in range(4):
+        assert np.array_equal(soa[a], np.concatenate([t[a] for t in tracks]))
+    # the folder loop makes one task per track, empty ones included, with cumulative entry points
+    tasks = st.macro_tasks(_macro(tmp_path))
+    assert [(t["entry"], t["exit"]) for t in tasks] == [(0, 3), (3, 3), (3, 10), (10, 11)]
+
+
+def test_corrupt_track_files_are_config_errors(tmp_path):
+    rs = np.random.default_rng(6)
+    st.write_track_file(str(tmp_path / "f00.strk"),
+                        [tuple(rs.normal(size=n) for _ in range(4)) for n in (4, 6)])
+    good = (tmp_path / "f00.strk").read_bytes()
+    bad_files = [b"XXXXv001" + good[8:],                                    # wrong magic
+                 good[:20],                                                 # short header
+                 good[:24] + np.array([6, 4], "<u8").tobytes() + good[40:],  # index decreases
+                 good[:24] + np.array([4, 11], "<u8").tobytes() + good[40:]]  # index past the end
+    for bad in bad_files:
+        (tmp_path / "f00.strk").write_bytes(bad)
+        with pytest.raises(st.StError) as e:
+            st.macro_tasks(_macro(tmp_path))
+        assert e.value.status == _capi.ST_ERR_CONFIG
+
+
 def test_macro_errors(tmp_path):
     p = tmp_path / "bad.ini"
     p.write_text("[Run]\nType = File\nPath = /x\n")
