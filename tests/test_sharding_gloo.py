@@ -1,4 +1,4 @@
-"""Multi-rank sharding logic on CPU: two gloo ranks each take their LPT share of the jobs, compute
+"""Multi-rank sharding logic on CPU: gloo ranks each take their LPT share of the jobs, compute
 their spectra (with the CPU oracle standing in for the GPU of each rank), and all-reduce them;
 the result equals the single-process spectrum of all jobs."""
 import os
@@ -23,7 +23,7 @@ def test_lpt_balances_and_covers():
     assert np.array_equal(lpt_assign(costs, 4), lpt_assign(costs, 4))  # deterministic
 
 
-def _worker(rank, world, store_path, out_path):
+def _worker(rank, world, store_path, out_path, n_tracks=12):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
@@ -36,7 +36,7 @@ def _worker(rank, world, store_path, out_path):
     dist.init_process_group("gloo", init_method="file://" + store_path, rank=rank,
                             world_size=world)
     try:
-        w = W.config0(n_tracks=12, n_os=3)
+        w = W.config0(n_tracks=n_tracks, n_os=3)
         costs = w.sizes * w.n_os
         e = po.edges(*w.hists[0])
         counts = np.zeros(len(e) - 1, dtype=np.int64)
@@ -53,20 +53,27 @@ def _worker(rank, world, store_path, out_path):
         dist.destroy_process_group()
 
 
-def test_two_rank_spectrum_equals_single_process(tmp_path):
+@pytest.mark.parametrize("world,n_tracks", [(2, 12), (3, 2)])
+def test_ranks_spectrum_equals_single_process(tmp_path, world, n_tracks):
+    """Two ranks sharing 12 tracks, and three ranks with two tracks (one rank has no job but
+    still takes part in the reduction)."""
     import pyoracle as po
     import supertrack_b200.workloads as W
+    from supertrack_b200.sharding import shard
+    w = W.config0(n_tracks=n_tracks, n_os=3)
+    owned = [len(shard(w.sizes * w.n_os, r, world)) for r in range(world)]
+    assert sum(owned) == w.n_jobs and (n_tracks >= world or 0 in owned)
     out = str(tmp_path / "r.npz")
     ctx = mp.get_context("spawn")
     store = str(tmp_path / "store")
-    procs = [ctx.Process(target=_worker, args=(r, 2, store, out)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, store, out, n_tracks))
+             for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
         p.join(timeout=300)
         assert p.exitcode == 0
     got = np.load(out)
-    w = W.config0(n_tracks=12, n_os=3)
     e = po.edges(*w.hists[0])
     counts = np.zeros(len(e) - 1, dtype=np.int64)
     yfy = np.zeros(len(e) - 1)
