@@ -309,6 +309,7 @@ class Context:
         self._check(lib().st_hist_read(self._h, hist, counts_ptr, yfy_ptr), "st_hist_read")
 
     def reset_histogram(self, hist: int = -1) -> None:
+        """Zeroes one histogram's counts and y*f(y) (all histograms for -1); ids stay valid."""
         self._check(lib().st_hist_reset(self._h, hist), "st_hist_reset")
 
     def total_bins(self) -> int:
@@ -344,6 +345,8 @@ class Context:
         v = _capi.st_track_view()
         if on_device:
             ptrs = [a if isinstance(a, int) else a.data_ptr() for a in (x, y, z, edep)]
+            if n is None and isinstance(x, int):
+                raise ValueError("n (deposits) is required with raw device pointers")
             nn = n if n is not None else int(x.numel())
             self._keep.extend([x, y, z, edep])
         else:
@@ -394,6 +397,9 @@ class Context:
         self._check(lib().st_run_finish(self._h), "st_run_finish")
 
     def clear_histograms(self) -> None:
+        """Deletes every histogram of the context: their ids become invalid, and a run of jobs
+        that still refer to them is refused. To zero the spectra instead, use
+        :meth:`reset_histogram`."""
         self._check(lib().st_hists_clear(self._h), "st_hists_clear")
 
     def run_export(self, cap: int = 1 << 20) -> np.ndarray:
