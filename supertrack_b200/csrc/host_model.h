@@ -8,6 +8,14 @@
 #include <string>
 #include <vector>
 
+// The library builds with hidden visibility; the C ABI and the C++ surface marked ST_CXX_API (this
+// header and supertrack.h) are what it exports, so C++ callers can link the classes directly.
+#if defined(__GNUC__)
+#define ST_CXX_API __attribute__((visibility("default")))
+#else
+#define ST_CXX_API
+#endif
+
 namespace st {
 
 // ---------------------------------------------------------------------------------------------
@@ -19,7 +27,7 @@ namespace st {
 // true/yes/on/1 and false/no/off/0 (:429-440). ParseError() is 0, the first bad line, or -1 when
 // the file cannot be opened.
 // ---------------------------------------------------------------------------------------------
-class INIReader {
+class ST_CXX_API INIReader {
  public:
   explicit INIReader(const std::string& filename);
   static INIReader FromString(const std::string& text);
@@ -49,9 +57,9 @@ class INIReader {
 // are log10 values stored as float. Returns false for an unknown type, nbins < 1, or edges that
 // are not finite and strictly increasing (for example a log histogram with a bound <= 0).
 // ---------------------------------------------------------------------------------------------
-void LinSpace(float bottom, float top, int nbins, double* bins);
-void LogSpace(float bottom, float top, int nbins, double* bins);
-bool MakeEdges(int type, int nbins, float lower, float upper, std::vector<double>* edges);
+ST_CXX_API void LinSpace(float bottom, float top, int nbins, double* bins);
+ST_CXX_API void LogSpace(float bottom, float top, int nbins, double* bins);
+ST_CXX_API bool MakeEdges(int type, int nbins, float lower, float upper, std::vector<double>* edges);
 
 // ---------------------------------------------------------------------------------------------
 // Spectrum post-processing (CPUHistogramUtils, utils.cc:37-117). The reference applies these to
@@ -63,17 +71,17 @@ bool MakeEdges(int type, int nbins, float lower, float upper, std::vector<double
 // ---------------------------------------------------------------------------------------------
 namespace CPUHistogramUtils {
 // Edges of an axis given in log10 units: 10^(from + i * (to - from) / nbins), i = 0..nbins.
-void BinLogX(int nbins, double from, double to, double* edges);
+ST_CXX_API void BinLogX(int nbins, double from, double to, double* edges);
 // Counts per bin to a normalised density (divide by bin width, then by the count total).
-void PMF_to_PDF(int nbins, const double* edges, double* contents);
+ST_CXX_API void PMF_to_PDF(int nbins, const double* edges, double* contents);
 // Density to y*f(y) (multiply by the bin midpoint).
-void Prepare_for_Semilog(int nbins, const double* edges, double* contents);
+ST_CXX_API void Prepare_for_Semilog(int nbins, const double* edges, double* contents);
 }  // namespace CPUHistogramUtils
 
 // ---------------------------------------------------------------------------------------------
 // Tasks and their seeds (ThreadTask.hh:6-31, ThreadAllocation.cc:16-32, ThreadAllocator.cc).
 // ---------------------------------------------------------------------------------------------
-struct ThreadTask {
+struct ST_CXX_API ThreadTask {
   std::string fileName;
   int64_t entryPoint = 0;   // first deposit of the track in the file
   int64_t exitPoint = 0;    // one past the last deposit
@@ -83,7 +91,7 @@ struct ThreadTask {
   int32_t trackInFile = 0;
 };
 
-struct ThreadAllocation {
+struct ST_CXX_API ThreadAllocation {
   int32_t threadID = 0;
   int64_t randomSeed = 0;
   int32_t nOversamples = 1;
@@ -93,7 +101,7 @@ struct ThreadAllocation {
   bool AddTask(const ThreadTask& task);
 };
 
-struct RunConfig {
+struct ST_CXX_API RunConfig {
   std::string type;
   std::string path;
   long firstFile = -1;
@@ -105,11 +113,11 @@ struct RunConfig {
 
 // Reads the [Run] keys (ThreadAllocator.cc:29-49). RandomSeed -1 becomes time(NULL).
 // Returns an empty string on success or the reason the macro is unusable.
-std::string ReadRunConfig(const INIReader& reader, RunConfig* cfg);
+ST_CXX_API std::string ReadRunConfig(const INIReader& reader, RunConfig* cfg);
 
 // Folder enumeration, file limits, one task per track and the contiguous split over threads
 // (ThreadAllocator.cc:51-133). Returns an empty string on success or the error text.
-std::string ReturnThreadAllocations(const RunConfig& cfg, std::vector<ThreadAllocation>* out);
+ST_CXX_API std::string ReturnThreadAllocations(const RunConfig& cfg, std::vector<ThreadAllocation>* out);
 
 // ---------------------------------------------------------------------------------------------
 // Track files. One file holds several tracks as float64 SoA deposits plus the cumulative end
@@ -122,10 +130,10 @@ std::string ReturnThreadAllocations(const RunConfig& cfg, std::vector<ThreadAllo
 //   then       : float64  x[n], y[n], z[n], edep[n]
 // ---------------------------------------------------------------------------------------------
 constexpr const char* kTrackFileExtension = ".strk";
-bool ReadTrackIndex(const std::string& path, std::vector<uint64_t>* index, uint64_t* n_deposits);
-bool ReadTrackDeposits(const std::string& path, int64_t begin, int64_t end, double* x, double* y,
+ST_CXX_API bool ReadTrackIndex(const std::string& path, std::vector<uint64_t>* index, uint64_t* n_deposits);
+ST_CXX_API bool ReadTrackDeposits(const std::string& path, int64_t begin, int64_t end, double* x, double* y,
                        double* z, double* edep);
-bool WriteTrackFile(const std::string& path, uint64_t n_tracks, const uint64_t* index,
+ST_CXX_API bool WriteTrackFile(const std::string& path, uint64_t n_tracks, const uint64_t* index,
                     uint64_t n_deposits, const double* x, const double* y, const double* z,
                     const double* edep);
 

@@ -24,7 +24,7 @@
 namespace st {
 
 // SphericalGeometry (SphericalGeometry.cuh:8-23) constructed from (HL, d) or the macro.
-struct SphericalGeometry {
+struct ST_CXX_API SphericalGeometry {
   SphericalGeometry(double scoring_region_half_length, double sphere_diameter);
   explicit SphericalGeometry(const INIReader& reader);
   double scoringRegionLength = 0;
@@ -38,7 +38,7 @@ struct SphericalGeometry {
 
 // Host-resident SoA track (Track.cuh:7-22); AllocateAndLoadTrack reads a task's deposits from
 // its track file.
-class Track {
+class ST_CXX_API Track {
  public:
   bool AllocateAndLoadTrack(const ThreadTask& task);
   void Free();
@@ -50,7 +50,7 @@ class SimulationMethod;
 
 // The per-track hand-off between the simulation method and the histogram (VolumeEdepPair.cuh).
 // It records which oversamples of which track are pending instead of holding per-hit pairs.
-class VolumeEdepPair {
+class ST_CXX_API VolumeEdepPair {
  public:
   void Allocate(uint64_t /*numInputElements*/) { pending = 0; }
   void Free() { pending = 0; }
@@ -59,7 +59,7 @@ class VolumeEdepPair {
   uint32_t pending = 0;
 };
 
-class SimulationMethod {
+class ST_CXX_API SimulationMethod {
  public:
   explicit SimulationMethod(const INIReader& macroReader) : _macroReader(macroReader) {}
   virtual ~SimulationMethod() = default;
@@ -79,7 +79,7 @@ using SimulationMethodCtor = SimulationMethod* (*)(const INIReader&);
 
 // Name -> constructor registry (SimulationMethodFactory.hh:12-37). Construct returns nullptr when
 // no registered name matches [Simulation] Method.
-class SimulationMethodFactory {
+class ST_CXX_API SimulationMethodFactory {
  public:
   static SimulationMethodFactory& GetInstance();
   void AddSimulationMethod(const std::string& name, SimulationMethodCtor ctor);
@@ -96,7 +96,7 @@ class SimulationMethodFactory {
 // added ZOriginShift = plus|minus|none (default plus, the reference's +HL'). The
 // SuggestedCudaBlocks/Threads keys are accepted and ignored: the fused kernel picks its own
 // launch shape.
-class VoxelConstrainedSphereMethod : public SimulationMethod {
+class ST_CXX_API VoxelConstrainedSphereMethod : public SimulationMethod {
  public:
   explicit VoxelConstrainedSphereMethod(const INIReader& macroReader);
   static SimulationMethod* Construct(const INIReader& macroReader);
@@ -120,7 +120,7 @@ class VoxelConstrainedSphereMethod : public SimulationMethod {
 
 // Histogram (Histogram.cuh:15-72) over a shared GPU context. f(y) counts are exact int64 sums;
 // y*f(y) is a float64 sum per bin.
-class Histogram {
+class ST_CXX_API Histogram {
  public:
   Histogram(int nbins, float binLower, float binUpper, const std::string& type, st_ctx* ctx);
   Histogram(const INIReader& reader, st_ctx* ctx);
@@ -150,7 +150,7 @@ class Histogram {
 
 // SuperTrackManager (SuperTrackManager.hh). Run() loads every task's track and runs all of them
 // as one batched launch per memory-bounded group of tracks, summing into one spectrum.
-class SuperTrackManager {
+class ST_CXX_API SuperTrackManager {
  public:
   static SuperTrackManager& GetInstance();
   void AddSimulationMethod(const std::string& name, SimulationMethodCtor ctor);

@@ -326,6 +326,94 @@ def test_corrupt_track_files_are_config_errors(tmp_path):
         assert e.value.status == _capi.ST_ERR_CONFIG
 
 
+CXX_PROGRAM = r"""
+#include <cstdio>
+#include <string>
+#include "supertrack.h"
+
+// The reference's C++ route up to the GPU launch, linked against libsupertrack_b200.so.
+int main(int argc, char** argv) {
+  st::SphericalGeometry g(2500.0, 10.0);
+  st_geometry c;
+  if (st_geometry_make(2500.0, 10.0, &c) != ST_OK) return 2;
+  std::printf("geometry %d %.17g %.17g %d\n", g.numSpheresLinear, g.greatestSphereOffset,
+              g.scoringRegionHalfLength, c.num_spheres_linear == g.numSpheresLinear);
+  st::INIReader r = st::INIReader::FromString("[Histogram]\nNBins = 3000 ; bins\n");
+  std::printf("nbins %ld\n", r.GetInteger("Histogram", "NBins", 0));
+  st::SuperTrackManager& mgr = st::SuperTrackManager::GetInstance();
+  mgr.AddSimulationMethod("VoxelConstrainedSphere", &st::VoxelConstrainedSphereMethod::Construct);
+  const std::string e = mgr.Initialize(argv[1]);
+  if (!e.empty()) {
+    std::printf("error %s\n", e.c_str());
+    return 3;
+  }
+  st::INIReader macro(argv[1]);
+  st::SimulationMethodFactory& f = st::SimulationMethodFactory::GetInstance();
+  f.AddSimulationMethod("VoxelConstrainedSphere", &st::VoxelConstrainedSphereMethod::Construct);
+  st::SimulationMethod* m = f.Construct(macro);
+  auto* vcs = dynamic_cast<st::VoxelConstrainedSphereMethod*>(m);
+  if (!vcs) return 4;
+  std::printf("method %d %d\n", vcs->Geometry().numSpheresLinear, (int)vcs->ShiftTrack());
+  long tasks = 0;
+  double sum = 0;
+  for (const auto& a : mgr.Allocations())
+    for (const auto& t : a.tasks) {
+      st::Track track;
+      if (!track.AllocateAndLoadTrack(t)) return 5;
+      for (int64_t i = 0; i < track.Size(); ++i) sum += track.edep[i];
+      ++tasks;
+    }
+  std::printf("tasks %ld %.17g\n", tasks, sum);
+  delete m;
+  return 0;
+}
+"""
+
+
+def test_cpp_surface_links_and_runs_the_host_side(tmp_path):
+    """A C++ caller of the reference's classes (SphericalGeometry, INIReader,
+    SimulationMethodFactory, VoxelConstrainedSphereMethod, SuperTrackManager, Track) compiles
+    against the shipped headers, links libsupertrack_b200.so alone, and gets the same geometry,
+    tasks and deposits as the Python surface (everything before the GPU launch)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "supertrack_b200")
+    src = tmp_path / "route.cc"
+    src.write_text(CXX_PROGRAM)
+    exe = tmp_path / "route"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-o", str(exe), str(src),
+                    "-I", os.path.join(root, "supertrack_b200", "csrc"),
+                    "-L", libdir, "-lsupertrack_b200", "-Wl,-rpath," + libdir],
+                   check=True, capture_output=True, text=True)
+    folder = tmp_path / "tracks"
+    folder.mkdir()
+    _write_folder(folder, [3, 2])
+    out = subprocess.run([str(exe), _macro(folder, Threads=2)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    lines = dict(l.split(" ", 1) for l in out.stdout.strip().splitlines())
+    g = st.geometry(2500.0, 10.0)
+    n, gso, hl, same = lines["geometry"].split()
+    assert int(n) == g["num_spheres_linear"] and float(gso) == g["greatest_sphere_offset"]
+    assert float(hl) == g["scoring_region_half_length"] and same == "1"
+    assert lines["nbins"] == "3000"
+    assert lines["method"].split() == [str(st.geometry(100.0, 10.0)["num_spheres_linear"]), "1"]
+    tasks = st.macro_tasks(_macro(folder, Threads=2))
+    total = 0.0
+    rs = np.random.default_rng(0)                 # the deposits _write_folder generated
+    for nt in (3, 2):
+        for _ in range(nt):
+            m = int(rs.integers(1, 50))
+            arrs = [rs.normal(size=m) for _ in range(4)]
+            for v in arrs[3]:
+                total += v
+    nt_out, s_out = lines["tasks"].split()
+    assert int(nt_out) == len(tasks) == 5
+    assert float(s_out) == total
+
+
 def test_macro_errors(tmp_path):
     p = tmp_path / "bad.ini"
     p.write_text("[Run]\nType = File\nPath = /x\n")
