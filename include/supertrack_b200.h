@@ -361,7 +361,9 @@ typedef struct {
 /* SuperTrackManager::Initialize(new INIReader(path)) + Run() (SuperTrackManager.cu:28-102):
  * reads the macro, enumerates the track folder, derives the task seeds, runs every task on
  * the GPU and writes <[Output] Path><NamePrefix><seed>.csv/.json unless write_output == 0.
- * counts/yfy receive the summed spectrum (nbins_cap entries available). */
+ * counts/yfy receive the summed spectrum (nbins_cap entries available). A macro or track folder
+ * that cannot be used returns ST_ERR_CONFIG; a failed library call returns its own status (for
+ * example ST_ERR_NO_DEVICE without a GPU, or a job's rejection); err receives the reason. */
 ST_API st_status st_run_macro(const char* ini_path, int32_t device, int32_t write_output,
                               int64_t* counts, double* yfy, int32_t nbins_cap,
                               st_run_info* info, char* err, size_t err_len);

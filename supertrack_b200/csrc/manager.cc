@@ -195,6 +195,7 @@ void SuperTrackManager::Reset() {
   _edges.clear();
   _deposits = 0;
   _initialized = false;
+  _runStatus = ST_OK;
 }
 
 std::string SuperTrackManager::Initialize(const std::string& iniPath, int device) {
@@ -213,12 +214,16 @@ std::string SuperTrackManager::Initialize(const std::string& iniPath, int device
 
 std::string SuperTrackManager::Run(bool writeOutput) {
   if (!_initialized) return "Can not start run without initializing manager.";
+  _runStatus = ST_OK;
   std::unique_ptr<SimulationMethod> method(SimulationMethodFactory::GetInstance().Construct(_reader));
   if (!method)
     return "No simulation method matching name: " + _reader.Get("Simulation", "Method", "") + " found.";
   st_ctx* ctx = nullptr;
   st_status s = st_ctx_create(_device, nullptr, &ctx);
-  if (s != ST_OK) return std::string("GPU context: ") + st_status_string(s);
+  if (s != ST_OK) {
+    _runStatus = s;
+    return std::string("GPU context: ") + st_status_string(s);
+  }
   std::string err;
   {
     Histogram histogram(_reader, ctx);
@@ -241,6 +246,7 @@ std::string SuperTrackManager::Run(bool writeOutput) {
         char buf[256];
         st_ctx_last_error(ctx, buf, sizeof(buf));
         err = std::string("GPU run failed: ") + st_status_string(rs) + " " + buf;
+        _runStatus = rs;
         return false;
       }
       return true;
@@ -258,7 +264,11 @@ std::string SuperTrackManager::Run(bool writeOutput) {
         v.x = track->x.data(); v.y = track->y.data(); v.z = track->z.data(); v.edep = track->edep.data();
         v.n = track->Size();
         s = st_job_submit(ctx, &v, &d, nullptr);
-        if (s != ST_OK) { err = std::string("Job rejected: ") + st_status_string(s); break; }
+        if (s != ST_OK) {
+          err = std::string("Job rejected: ") + st_status_string(s);
+          _runStatus = s;
+          break;
+        }
         method->FreeTrackProcess();
         _deposits += track->Size();
         group_deposits += track->Size();
@@ -330,8 +340,8 @@ st_status st_run_macro(const char* ini_path, int32_t device, int32_t write_outpu
   if (!e.empty()) return fail(ST_ERR_CONFIG, e);
   e = mgr.Run(write_output != 0);
   if (!e.empty()) {
-    const bool gpu = e.rfind("GPU", 0) == 0;
-    return fail(gpu ? ST_ERR_CUDA : ST_ERR_CONFIG, e);
+    const st_status g = mgr.RunStatus();
+    return fail(g != ST_OK ? g : ST_ERR_CONFIG, e);
   }
   const auto& c = mgr.GetOutputCounts();
   const auto& y = mgr.GetOutputYFY();

@@ -162,6 +162,9 @@ class ST_CXX_API SuperTrackManager {
   const std::vector<double>& GetOutputEdges() const { return _edges; }
   const std::vector<ThreadAllocation>& Allocations() const { return _threadAllocations; }
   int64_t Deposits() const { return _deposits; }
+  // Status of the library call (context, job submit, GPU run) that stopped the last Run; ST_OK
+  // when none did, including when Run stopped on the macro or the track files instead.
+  st_status RunStatus() const { return _runStatus; }
   void Reset();
 
  private:
@@ -176,6 +179,7 @@ class ST_CXX_API SuperTrackManager {
   int64_t _deposits = 0;
   int _device = 0;
   bool _initialized = false;
+  st_status _runStatus = ST_OK;
 };
 
 }  // namespace st

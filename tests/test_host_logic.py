@@ -414,6 +414,32 @@ def test_cpp_surface_links_and_runs_the_host_side(tmp_path):
     assert float(s_out) == total
 
 
+def test_cli_reports_unusable_macros(tmp_path):
+    """`supertrack macro.ini` (SuperTrack.cu:9-36) exits 1 with the reason when the macro cannot
+    be used, before any GPU work."""
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "supertrack_b200", "supertrack")
+    if not os.path.exists(exe):
+        pytest.skip("the supertrack command is not built")
+    r = subprocess.run([exe, str(tmp_path / "none.ini")], capture_output=True, text=True)
+    assert r.returncode == 1 and "Cannot open macro file" in r.stderr
+    bad = tmp_path / "bad.ini"
+    bad.write_text("[Run]\nType = Folder\n")
+    r = subprocess.run([exe, str(bad)], capture_output=True, text=True)
+    assert r.returncode == 1 and "configuration error" in r.stderr
+
+
+def test_run_macro_without_device_reports_no_device(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    _write_folder(tmp_path, [2])
+    with pytest.raises(st.StError) as e:
+        st.run_macro(_macro(tmp_path), write_output=False)
+    assert e.value.status == _capi.ST_ERR_NO_DEVICE
+
+
 def test_macro_errors(tmp_path):
     p = tmp_path / "bad.ini"
     p.write_text("[Run]\nType = File\nPath = /x\n")
