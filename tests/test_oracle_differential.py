@@ -1,5 +1,6 @@
 """The C oracle against an independent pure-Python restatement of the reference's
-VoxelConstrainedSphere path, on small seeded tracks (CPU only).
+VoxelConstrainedSphere path, on small seeded tracks (CPU only); and the oracle's FP32 geometry
+variant against a numpy float32 restatement of it.
 
 The restatement follows the reference directly: geometry (SphericalGeometry.cu:7-32), z-origin
 shift (VoxelConstrainedSphereMethod.cu:138-154), XY shift and strict box test (:176-177, :198),
@@ -130,3 +131,59 @@ def test_oracle_matches_python_restatement(case):
         _, half_up = py_job(x, y, z, e, hl, d, zs, pts, edges,
                             rnd=lambda v: math.floor(v + 0.5))
         assert sorted(half_up) != sorted(rec)
+
+
+def py_job_f32(x, y, z, edep, hl, d, zshift, sxsy, edges):
+    """The FP32 geometry variant: x, y, the shifts and the voxel half-length rounded to float and
+    the box test in float; a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a and
+    dist = (dx^2 + dy^2) + float(dz^2) in float, with z, keys and values as in the FP64 path.
+    numpy float32 scalars round every operation and never contract to FMA."""
+    f = np.float32
+    g = py_geometry(hl, d)
+    hlp, gso, n, r2 = g["HL"], g["gSO"], g["N"], g["r"] * g["r"]
+    lineal = (2.0 / 3.0) * d
+    f_hl, f_gso, f_d, f_r2 = f(hlp), f(gso), f(d), f(r2)
+    f_inv_d = f(1.0) / f_d
+    zs = [float(v) + ZSHIFT[zshift] * hlp for v in z]
+    records = []
+    for os_, (sx, sy) in enumerate(sxsy):
+        spheres = {}
+        for i in range(len(x)):
+            fx, fy = f(x[i]) + f(sx), f(y[i]) + f(sy)
+            if not (abs(fx) < f_hl and abs(fy) < f_hl and abs(zs[i]) < hlp):
+                continue
+            ax, ay = fx - f_gso, fy - f_gso
+            kx, ky = np.rint(ax * f_inv_d), np.rint(ay * f_inv_d)
+            dx, dy = kx * f_d - ax, ky * f_d - ay
+            az = zs[i] - gso
+            kz = round(az / d)
+            dz = float(kz) * d - az
+            if (dx * dx + dy * dy) + f(dz * dz) <= f_r2:
+                key = (int(kx) + int(ky) * n + kz * n * n) % U64
+                spheres.setdefault(key, []).append(float(edep[i]) / lineal)
+        for key in sorted(spheres):
+            vals = spheres[key]
+            seq = vals[0]
+            for v in vals[1:]:
+                seq = seq + v
+            yx = math.fsum(vals)
+            b = int(np.searchsorted(edges, yx, side="right")) - 1
+            records.append((os_, key, len(vals), yx, seq, b if 0 <= b < len(edges) - 1 else -1))
+    return records
+
+
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] != "ties"], ids=lambda c: c[0])
+def test_fp32_oracle_matches_float32_restatement(case):
+    name, x, y, z, e, hl, d, zs, shift = case
+    n_os = 4
+    sx = po.shifts(hl, d, shift, 99, 3, n_os)
+    edges = po.edges("log", 60, 0.01, 1e4)
+    counts, yfy, stats, sph = po.run_job(x, y, z, e, half_length=hl, sphere_diameter=d, sxsy=sx,
+                                         edges_arr=edges, zshift=zs, spheres_cap=1 << 16,
+                                         precision=32)
+    rec = py_job_f32(x, y, z, e, hl, d, zs, [tuple(v) for v in sx], edges)
+    assert len(rec) > 0, name
+    got = sorted((int(s["os"]), int(s["key"]), int(s["nhits"]), float(s["y"]),
+                  float(s["y_seq"]), int(s["bin"])) for s in sph)
+    assert got == sorted(rec)
+    assert stats["hits"] == sum(r[2] for r in rec)
