@@ -1,19 +1,23 @@
 // st_superimpose_noalloc: one track's superimposition with no device allocation.
 //
-// Who needs it: callers that must not call cudaMalloc/cudaFree on their path — cudaFree
-// synchronises the whole device and stalls every other stream (a serving thread sharing the GPU
-// cannot afford that), many embedding frameworks own all device memory through their own pool,
-// and code that records work into CUDA graphs may not allocate between launches. The regular
-// entry points grow their arenas with cudaMalloc on first use; this one works entirely inside a
-// fixed scratch array that is part of the library image.
+// Who needs it: callers that must not call cudaMalloc/cudaFree on their path. cudaFree
+// synchronises the whole device and stalls every other stream, which a serving thread sharing the
+// GPU cannot afford; and frameworks that own all device memory through their own pool leave no
+// room for, or forbid, allocations of their plug-ins. The regular entry points grow their arenas
+// with cudaMalloc on first use; this one works entirely inside a fixed scratch array that is part
+// of the library image.
 //
 // The scratch below is a file-scope __device__ array: every GPU that loads the library holds it
 // (kScratchBytes, about 6.2 MB) until the process exits. Host code cannot pass the symbol
 // itself to a kernel (on the host it names a host-side stand-in), so the first call on each
-// device, with that device current, resolves its device address with cudaGetSymbolAddress; that
-// first call should therefore come before any stream capture. Every call shares the one array and
-// re-initialises the parts that must start empty (hash tables, counters, flags) itself, so calls
-// that overlap on the GPU race with each other: issue them on one stream, or serialise them.
+// device, with that device current, resolves its device address with cudaGetSymbolAddress and
+// sets the fused kernel's shared-memory attribute; that first call should therefore come before
+// any stream capture. Every call shares the one array and re-initialises the parts that must start
+// empty (hash tables, counters, flags) itself, so two calls whose work overlapped on the GPU would
+// race. Sharing a stream does not prevent that: the host-to-device copies of one call could be
+// enqueued between the copies and the kernels of another. Calls are therefore serialised on the
+// host: each holds a per-device lock from its first enqueue until its final stream
+// synchronisation, and returns only after its work on the GPU has finished.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,6 +47,10 @@ constexpr int kNaGrid = 4;                      // resident CTAs (and spill tabl
 constexpr uint32_t kNaTableCap = 2 * kNaMaxDeposits;   // spill-table slots (power of two)
 constexpr uint32_t kNaCellCap = 2 * kNaMaxDeposits;    // cell-hash slots (power of two)
 constexpr int64_t kNaBlocks = kNaMaxDeposits / st::kPrepSlotsPerBlock;
+// planning parameters: the regular context's defaults
+constexpr int64_t kNaFlagMinKept = 16384;       // window flags only above this many kept deposits
+constexpr int64_t kNaItemCost = 1 << 18;        // deposit*oversamples per private work item
+constexpr int kNaChunkWindows = 4;              // windows per chunk (shared units; none here)
 
 constexpr size_t al(size_t v) { return (v + 255) / 256 * 256; }
 
@@ -96,6 +104,8 @@ constexpr size_t kScratchBytes = kLayout.total;
 std::mutex g_setup_mu;
 constexpr int kMaxDevices = 64;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
+// held by a call from its first enqueue to its final synchronisation (one scratch per device)
+std::mutex g_call_mu[kMaxDevices];
 
 }  // namespace
 
@@ -154,6 +164,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   unsigned char* base = nullptr;
   st_status s = noalloc_setup(device, &base);
   if (s != ST_OK) return s;
+  std::lock_guard<std::mutex> call_lock(g_call_mu[device]);
   const cudaStream_t st_ = (cudaStream_t)stream;
   const Layout& L = kLayout;
 
@@ -255,6 +266,10 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   pp.PVLO = (unsigned long long*)(base + L.pvlo);
   pp.PVHI = (unsigned long long*)(base + L.pvhi);
   pp.PKEY = (unsigned long long*)(base + L.pkey);
+  // the regular path's default: window flags only above this many kept deposits (a track here
+  // keeps at most kNaMaxDeposits, so the scratch path never runs windowed, as the regular path
+  // would not for the same track)
+  pp.flag_min_kept = kNaFlagMinKept;
 
   st::PlanParams q;
   std::memset(&q, 0, sizeof(q));
@@ -262,10 +277,13 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   q.jobs = pp.jobs;
   q.aux = pp.aux;
   q.n_jobs = 1;
-  q.chunk_windows = 4;
+  q.chunk_windows = kNaChunkWindows;
   q.max_helpers = 1;
   q.grid = kNaGrid;
-  q.item_cost = 1 << 18;
+  q.item_cost = kNaItemCost;
+  // deliberate difference from the regular path: share_divisor 0 (left zero) rules out shared
+  // units, whose helpers would need a spill table each from a pool sized for kNaGrid CTAs;
+  // min_chunks only matters for shared units
   q.total_units = (unsigned long long*)m;
   q.n_items = (int*)(m + 8);
   q.unit_counter = (unsigned int*)(m + 12);
@@ -297,7 +315,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   fp.unit_done = (unsigned int*)(base + L.units + 4);
   fp.unit_table = (int*)(base + L.units + 8);
   fp.pool_bits = (unsigned int*)(base + L.pool);
-  fp.chunk_windows = 4;
+  fp.chunk_windows = kNaChunkWindows;
 
   NA_CUDA(st::launch_prepare(pp, n_blocks, D.flagged != 0, st_));
   NA_CUDA(st::launch_plan(q, st_));
@@ -319,7 +337,10 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
         st::choose_grid_exponent(out.e_min, out.e_max, n, out.flags & st::kAuxNonzero);
     stats_out->status = (out.flags & st::kAuxNonfinite) ? ST_ERR_NONFINITE_EDEP : ST_OK;
   }
+  // after an error the caller's d_counts / d_yfy may hold part of this call's sums
   if (out.flags & st::kAuxNonfinite) return ST_ERR_NONFINITE_EDEP;
+  if (errflags[0] & 1) return ST_ERR_DEVICE_OVERFLOW;       // spill table full
+  if (errflags[0] & (4 | 8)) return ST_ERR_DEVICE_WAIT;     // pool exhausted / unit wait expired
   if (errflags[0]) return ST_ERR_DEVICE_OVERFLOW;
   return ST_OK;
 }
