@@ -147,6 +147,10 @@ ST_API st_status st_ctx_last_timing(const st_ctx* ctx, float* prepare_ms, float*
                                     int32_t* launches);
 /* Measured FP64 add/multiply issue rate of the device (operations per second). */
 ST_API st_status st_measure_fp64_peak(st_ctx* ctx, double* ops_per_second);
+/* Measured rate of conflict-free 64-bit shared-memory atomic additions of the device (one CTA
+ * of 1024 threads per SM, the fused kernel's shape), in atomics per second. No counterpart in the
+ * reference: the peak that the shared-memory roofline term of the fused kernel is set against. */
+ST_API st_status st_measure_smem_atomic_peak(st_ctx* ctx, double* atomics_per_second);
 /* Tuning knobs: target deposit*oversamples per work item, resident CTAs (0 = one per SM). */
 ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid);
 /* Named work-planning parameters (all take effect at the next run):
@@ -211,9 +215,9 @@ ST_API st_status st_hist_create(st_ctx* ctx, int32_t type, int32_t nbins, float 
 ST_API st_status st_hist_read(st_ctx* ctx, int32_t hist_id, int64_t* counts, double* yfy);
 /* Zeroes one histogram, or all of them with hist_id = -1. */
 ST_API st_status st_hist_reset(st_ctx* ctx, int32_t hist_id);
-/* Copies every histogram of the context in two transfers: counts/yfy receive all bins in
- * histogram creation order (st_hist_offset gives each histogram's first bin); cap is the room
- * in each array; n_bins receives the total. */
+/* Copies every histogram of the context in two transfers: counts/yfy (host or device memory)
+ * receive all bins in histogram creation order (st_hist_offset gives each histogram's first
+ * bin); cap is the room in each array; n_bins receives the total. */
 ST_API st_status st_hist_read_all(st_ctx* ctx, int64_t* counts, double* yfy, int64_t cap,
                                   int64_t* n_bins);
 ST_API st_status st_hist_offset(const st_ctx* ctx, int32_t hist_id, int64_t* first_bin);
@@ -328,18 +332,22 @@ ST_API st_status st_server_drain(st_server* server, int64_t timeout_ms);
 /* --- superimposition without device allocation ------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their
  * path: cudaFree synchronises the whole device and stalls every other stream (a serving thread
- * sharing the GPU cannot afford that), embedding frameworks often own all device memory through
- * their own pool, and work recorded into CUDA graphs may not allocate between launches. The call
- * allocates nothing: it works in a fixed scratch array compiled into the library
+ * sharing the GPU cannot afford that), and frameworks that own all device memory through their
+ * own pool leave no room for, or forbid, allocations by their plug-ins. The call allocates
+ * nothing: it works in a fixed scratch array compiled into the library
  * (st_noalloc_scratch_bytes() bytes, about 6.2 MB, held by every GPU that loads the library
  * until the process exits). Limits: one device-resident track (track->on_device != 0) of at
  * most 16384 deposits, at most 65536 oversamples, a histogram of at most 4096 bins; larger
  * requests return ST_ERR_CAPACITY. d_counts (int64) and d_yfy (float64) are device arrays of
- * nbins that the call adds into. desc->hist_id is ignored. Work is enqueued on `stream` (NULL:
- * the legacy default stream) on the current device, which is synchronised before returning.
- * The first call on each device resolves the scratch array's device address and should come
- * before any stream capture. All calls share the one scratch array, so calls that overlap on the
- * GPU race: issue them on one stream or serialise them. */
+ * nbins that the call adds into; after an error status they may hold part of the call's sums.
+ * desc->hist_id is ignored. Work is enqueued on `stream` (NULL: the legacy default stream) on the
+ * current device, and the call synchronises that stream before it returns.
+ * The first call on each device resolves the scratch array's device address (and sets a kernel
+ * attribute), so that first call should come before any stream capture. All calls share the one
+ * scratch array, and two calls whose GPU work overlapped would race; a shared stream does not
+ * prevent that, since one call's copies could be enqueued between another's copies and kernels.
+ * The library therefore serialises the calls of a process per device: each call holds a lock
+ * from its first enqueue to its final synchronisation. */
 ST_API st_status st_superimpose_noalloc(const st_track_view* track, const st_job_desc* desc,
                                         int32_t hist_type, int32_t nbins, float lower,
                                         float upper, int64_t* d_counts, double* d_yfy,

@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 OR_SUM_EXACT = 0
 OR_SUM_SEQ = 1
 
+STATS_DTYPE = np.dtype([("hits", "<i8"), ("spheres", "<i8"), ("binned", "<i8"),
+                        ("grid_exponent", "<i4"), ("status", "<i4")])
 SPHERE_DTYPE = np.dtype([("key", "<u8"), ("y", "<f8"), ("y_seq", "<f8"), ("nhits", "<i8"),
                          ("os", "<i4"), ("bin", "<i4")])
 
@@ -63,7 +65,7 @@ def lib() -> C.CDLL:
         h.or_job.restype = C.c_int
         h.or_job_f32.argtypes = h.or_job.argtypes
         h.or_job_f32.restype = C.c_int
-        h.or_run_batch.argtypes = [C.c_int64] + [C.c_void_p] * 20 + [C.c_int32]
+        h.or_run_batch.argtypes = [C.c_int64] + [C.c_void_p] * 22 + [C.c_int32]
         h.or_run_batch.restype = C.c_int
         _lib = h
     return _lib
@@ -147,9 +149,11 @@ def run_job(x, y, z, edep, *, half_length, sphere_diameter, sxsy, edges_arr, zsh
 
 
 def run_batch(x, y, z, edep, off, n, hl, d, zshift, shift_track, n_os, seed, track_id, hist,
-              edges_list, threads=1):
-    """Many jobs on `threads` host threads. edges_list[h] are the edges of histogram h.
-    Returns (counts list, yfy list)."""
+              edges_list, threads=1, job_stats=False):
+    """Many jobs on `threads` host threads, claimed in the given order. edges_list[h] are the
+    edges of histogram h. Returns (counts list, yfy list), plus, when job_stats is true, a
+    structured array of per-job (hits, spheres, binned, grid_exponent, status) and the thread
+    seconds of every job."""
     nb = np.array([len(e) - 1 for e in edges_list], dtype=np.int32)
     eoff = np.concatenate([[0], np.cumsum([len(e) for e in edges_list])[:-1]]).astype(np.int64)
     hoff = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.int64)
@@ -162,11 +166,14 @@ def run_batch(x, y, z, edep, off, n, hl, d, zshift, shift_track, n_os, seed, tra
             a(zshift, np.int32), a(shift_track, np.int32), a(n_os, np.uint32),
             a(seed, np.uint64), a(track_id, np.uint64), a(hist, np.int32), E, eoff, nb, hoff,
             counts, yfy]
-    failed = lib().or_run_batch(len(args[4]), *[_p(v) for v in args], threads)
+    js = np.zeros(len(args[4]), dtype=STATS_DTYPE)
+    secs = np.zeros(len(args[4]), dtype=np.float64)
+    failed = lib().or_run_batch(len(args[4]), *[_p(v) for v in args], _p(js), _p(secs), threads)
     if failed:
         raise RuntimeError(f"{failed} oracle jobs failed")
-    return ([counts[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))],
-            [yfy[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))])
+    out = ([counts[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))],
+           [yfy[hoff[h]:hoff[h] + nb[h]] for h in range(len(nb))])
+    return out + (js, secs) if job_stats else out
 
 
 # ---------------------------------------------------------------------------------------------

@@ -38,6 +38,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <time.h>
 
 #define OR_SUM_EXACT 0
 #define OR_SUM_SEQ 1
@@ -400,7 +401,10 @@ int or_job_f32(const double* x, const double* y, const double* z, const double* 
  * Many jobs, threads over jobs (the CPU baseline). Job j reads deposits [off[j], off[j]+n[j])
  * of the SoA arrays, geometry (hl[j], d[j]), its own shifts from the Philox contract, and adds
  * into histogram hist[j] (counts/yfy laid out hist-major, nbins[h] bins at hoff[h], edges at
- * eoff[h]). Threads claim jobs from a shared counter. Returns the number of failed jobs.
+ * eoff[h]). Threads claim jobs from a shared counter in the given order (callers pass the
+ * largest first). job_stats (may be NULL) receives each job's hits, spheres and binned spheres;
+ * job_seconds (may be NULL) the thread time each job took (CLOCK_MONOTONIC around it, measured
+ * while the other threads work on their own jobs). Returns the number of failed jobs.
  */
 typedef struct {
   int64_t n_jobs;
@@ -417,6 +421,8 @@ typedef struct {
   const int64_t* hoff;
   int64_t* counts;
   double* yfy;
+  or_stats* job_stats;
+  double* job_seconds;
   int64_t next;
   int failed;
   pthread_mutex_t lock;
@@ -427,6 +433,8 @@ static void* batch_worker(void* arg) {
   for (;;) {
     int64_t j = __atomic_fetch_add(&B->next, 1, __ATOMIC_RELAXED);
     if (j >= B->n_jobs) break;
+    struct timespec t0, t1;
+    clock_gettime(CLOCK_MONOTONIC, &t0);
     or_geom g;
     int rc = or_geometry(B->hl[j], B->d[j], &g);
     if (!rc) {
@@ -434,10 +442,13 @@ static void* batch_worker(void* arg) {
       double* sxsy = (double*)malloc(sizeof(double) * 2 * (B->n_os[j] ? B->n_os[j] : 1));
       int64_t* c = (int64_t*)calloc((size_t)B->nbins[h], sizeof(int64_t));
       double* w = (double*)calloc((size_t)B->nbins[h], sizeof(double));
+      or_stats js;
+      memset(&js, 0, sizeof(js));
       or_shifts(&g, B->shift_track[j], B->seed[j], B->track_id[j], 0, B->n_os[j], sxsy);
       rc = or_job(B->x + B->off[j], B->y + B->off[j], B->z + B->off[j], B->edep + B->off[j],
                   B->n[j], B->hl[j], B->d[j], B->zshift[j], B->n_os[j], sxsy,
-                  B->edges + B->eoff[h], B->nbins[h], OR_SUM_EXACT, c, w, NULL, NULL, 0, NULL);
+                  B->edges + B->eoff[h], B->nbins[h], OR_SUM_EXACT, c, w, &js, NULL, 0, NULL);
+      if (B->job_stats) B->job_stats[j] = js;
       pthread_mutex_lock(&B->lock);
       for (int b = 0; b < B->nbins[h]; b++) {
         B->counts[B->hoff[h] + b] += c[b];
@@ -446,6 +457,9 @@ static void* batch_worker(void* arg) {
       pthread_mutex_unlock(&B->lock);
       free(c); free(w); free(sxsy);
     }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    if (B->job_seconds)
+      B->job_seconds[j] = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
     if (rc) __atomic_fetch_add(&B->failed, 1, __ATOMIC_RELAXED);
   }
   return NULL;
@@ -457,9 +471,10 @@ int or_run_batch(int64_t n_jobs, const double* x, const double* y, const double*
                  const uint32_t* n_os, const uint64_t* seed, const uint64_t* track_id,
                  const int32_t* hist, const double* edges, const int64_t* eoff,
                  const int32_t* nbins, const int64_t* hoff, int64_t* counts, double* yfy,
-                 int32_t threads) {
+                 or_stats* job_stats, double* job_seconds, int32_t threads) {
   batch_t B = {n_jobs, x, y, z, edep, off, n, hl, d, zshift, shift_track, n_os, seed, track_id,
-               hist, edges, eoff, nbins, hoff, counts, yfy, 0, 0, PTHREAD_MUTEX_INITIALIZER};
+               hist, edges, eoff, nbins, hoff, counts, yfy, job_stats, job_seconds, 0, 0,
+               PTHREAD_MUTEX_INITIALIZER};
   if (threads < 1) threads = 1;
   pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)threads);
   int started = 0;

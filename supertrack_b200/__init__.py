@@ -337,6 +337,13 @@ class Context:
         self._check(lib().st_measure_fp64_peak(self._h, C.byref(v)), "st_measure_fp64_peak")
         return v.value
 
+    def smem_atomic_peak(self) -> float:
+        """Measured conflict-free 64-bit shared-memory atomic additions per second."""
+        v = C.c_double()
+        self._check(lib().st_measure_smem_atomic_peak(self._h, C.byref(v)),
+                    "st_measure_smem_atomic_peak")
+        return v.value
+
     # jobs -----------------------------------------------------------------------------------
     def submit(self, x, y, z, edep, *, half_length: float, sphere_diameter: float,
                n_oversamples: int, hist: int, seed: int = 0, track_id: int = 0,

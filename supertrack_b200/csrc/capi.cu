@@ -20,6 +20,7 @@ cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_fl
 cudaError_t configure_fused();
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
+cudaError_t launch_smem_atomic_probe(unsigned long long* out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
 cudaError_t launch_reset_aux(JobAux* aux, int n, cudaStream_t s);
 }  // namespace st
@@ -1279,8 +1280,10 @@ st_status st_hist_read_all(st_ctx* c, int64_t* counts, double* yfy, int64_t cap,
   if (!counts && !yfy) return ST_OK;
   if (cap < c->h_bins) return ST_ERR_CAPACITY;
   if (c->h_bins == 0) return ST_OK;
-  if (counts) ST_CUDA(cudaMemcpyAsync(counts, c->h_counts.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
-  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, c->h_yfy.p, (size_t)c->h_bins * 8, cudaMemcpyDeviceToHost, c->stream), "histogram read");
+  // cudaMemcpyDefault: the destination may be host memory or device memory (a multi-GPU
+  // caller gathers the spectra in a device buffer for its all-reduce)
+  if (counts) ST_CUDA(cudaMemcpyAsync(counts, c->h_counts.p, (size_t)c->h_bins * 8, cudaMemcpyDefault, c->stream), "histogram read");
+  if (yfy) ST_CUDA(cudaMemcpyAsync(yfy, c->h_yfy.p, (size_t)c->h_bins * 8, cudaMemcpyDefault, c->stream), "histogram read");
   ST_CUDA(cudaStreamSynchronize(c->stream), "histogram read");
   return ST_OK;
 }
@@ -1463,6 +1466,28 @@ st_status st_measure_fp64_peak(st_ctx* c, double* ops_per_second) {
   release(out);
   // two FP64 operations (one multiply, one add) per chain step
   *ops_per_second = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (best * 1e-3);
+  return ST_OK;
+}
+
+st_status st_measure_smem_atomic_peak(st_ctx* c, double* atomics_per_second) {
+  if (!c || !atomics_per_second) return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  DevBuf out;
+  ST_CUDA(ensure(out, (size_t)c->sm_count * 8), "smem probe buffer");
+  const int blocks = c->sm_count, iters = 8192;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    ST_CUDA(cudaEventRecord(c->ev[0], c->stream), "event");
+    ST_CUDA(st::launch_smem_atomic_probe((unsigned long long*)out.p, blocks, iters, c->stream),
+            "smem probe");
+    ST_CUDA(cudaEventRecord(c->ev[1], c->stream), "event");
+    ST_CUDA(cudaEventSynchronize(c->ev[1]), "smem probe");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  release(out);
+  *atomics_per_second = (double)iters * 1024.0 * (double)blocks / (best * 1e-3);
   return ST_OK;
 }
 

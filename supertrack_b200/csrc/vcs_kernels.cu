@@ -1506,6 +1506,27 @@ cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s
 }
 
 // ---------------------------------------------------------------------------------------------
+// Shared-memory atomic probe: 64-bit atomic additions on a 4096-slot shared array, one CTA of
+// 1024 threads per SM (the fused kernel's shape). The lanes of a warp update consecutive slots
+// (no bank conflict beyond the two wavefronts a 64-bit warp access needs), so the rate is the
+// peak the fused kernel's per-hit and per-sphere shared-memory updates are set against.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024, 1) k_smem_atomic_probe(unsigned long long* out, int iters) {
+  __shared__ unsigned long long s[4096];
+  for (int i = threadIdx.x; i < 4096; i += blockDim.x) s[i] = 0;
+  __syncthreads();
+  const unsigned idx = threadIdx.x;  // 1024 distinct slots: lanes of a warp are consecutive
+  for (int i = 0; i < iters; ++i) atomicAdd(&s[(idx + (unsigned)i * 1024u) & 4095u], 1ull);
+  __syncthreads();
+  if (threadIdx.x == 0) out[blockIdx.x] = s[0] + s[4095];
+}
+
+cudaError_t launch_smem_atomic_probe(unsigned long long* out, int blocks, int iters, cudaStream_t s) {
+  k_smem_atomic_probe<<<blocks, 1024, 0, s>>>(out, iters);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
 // Host-side launch wrappers
 // ---------------------------------------------------------------------------------------------
 // 32 warps (64 registers each): the kernel is latency-bound, and more resident warps hide more

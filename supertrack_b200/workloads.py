@@ -16,9 +16,11 @@ Generators (all lengths in nm, energies in eV, float64):
            over [-HL, HL] and sorted; edep lognormal (median 20 eV, sigma 0.9) clipped to
            [10, 5000].
 
-Everything is vectorised over tracks with torch so that the large configurations can be
-generated on the GPU in well under a second; the same seed on the same device type gives the
-same tracks.
+Everything is vectorised with torch so that the large configurations can be generated on the
+GPU in seconds; the same seed on the same device type gives the same tracks. The single-geometry
+configurations (1 and 4) seed every track on its own (track t of seed s uses the generator
+seeded s * 1_000_003 + t), so a subset of their tracks is generated exactly as in the full
+workload, and the generator's temporaries stay at one track's size.
 """
 from __future__ import annotations
 
@@ -48,6 +50,7 @@ class Workload:
     hists: List[Tuple[str, int, float, float]] = field(default_factory=list)
     zshift: str = "none"
     shift_track: bool = True
+    generator: Optional[np.ndarray] = None   # int8 [n_jobs]: 0 proton-like, 1 ion-like
 
     @property
     def n_jobs(self) -> int:
@@ -67,6 +70,14 @@ class Workload:
         for k in ("x", "y", "z", "edep"):
             setattr(w, k, getattr(self, k).to(device))
         return w
+
+    def job_classes(self) -> np.ndarray:
+        """Class of every job, (generator, sphere diameter, oversamples) as one integer: jobs of
+        a class cost about the same per deposit*oversample."""
+        gen = self.generator if self.generator is not None else np.zeros(self.n_jobs, np.int8)
+        d_code = np.searchsorted(np.unique(self.diameter), self.diameter)
+        os_code = np.searchsorted(np.unique(self.n_os), self.n_os)
+        return (gen.astype(np.int64) * 64 + d_code) * 64 + os_code
 
     def job_arrays(self, j: int):
         o, n = int(self.offsets[j]), int(self.sizes[j])
@@ -168,7 +179,22 @@ def gen_ion(g, sizes: torch.Tensor, half_length: float, core_sigma: float, pen_m
     return pos[:, 0].contiguous(), pos[:, 1].contiguous(), pos[:, 2].contiguous(), edep
 
 
-def _assemble(name, parts, sizes, hl, d, n_os, seed, hists, hist_of_job) -> Workload:
+def _per_track(device, n_tracks, n_dep, seed, gen_one) -> Tuple[torch.Tensor, ...]:
+    """n_tracks tracks of n_dep deposits, track t generated by gen_one(generator, sizes) with a
+    generator seeded seed * 1_000_003 + t, written into preallocated arrays."""
+    total = n_tracks * n_dep
+    out = [torch.empty(total, dtype=torch.float64, device=device) for _ in range(4)]
+    sizes = torch.full((1,), n_dep, dtype=torch.long, device=device)
+    for t in range(n_tracks):
+        g = torch.Generator(device=device).manual_seed(seed * 1_000_003 + t)
+        part = gen_one(g, sizes)
+        for k in range(4):
+            out[k][t * n_dep:(t + 1) * n_dep] = part[k]
+        del part
+    return tuple(out)
+
+
+def _assemble(name, parts, sizes, hl, d, n_os, seed, hists, hist_of_job, generator=0) -> Workload:
     x = torch.cat([p[0] for p in parts])
     y = torch.cat([p[1] for p in parts])
     z = torch.cat([p[2] for p in parts])
@@ -182,7 +208,8 @@ def _assemble(name, parts, sizes, hl, d, n_os, seed, hists, hist_of_job) -> Work
                     n_os=np.broadcast_to(np.asarray(n_os, dtype=np.uint32), (nj,)).copy(),
                     seed=np.full(nj, seed, dtype=np.uint64),
                     track_id=np.arange(nj, dtype=np.uint64), hists=hists,
-                    hist_of_job=np.asarray(hist_of_job, dtype=np.int32))
+                    hist_of_job=np.asarray(hist_of_job, dtype=np.int32),
+                    generator=np.full(nj, generator, dtype=np.int8))
 
 
 def config0(device="cpu", n_tracks=64, n_dep=4000, n_os=10, seed=1) -> Workload:
@@ -198,11 +225,10 @@ def config0(device="cpu", n_tracks=64, n_dep=4000, n_os=10, seed=1) -> Workload:
 def config1(device="cpu", n_tracks=16, n_dep=1_000_000, n_os=100, seed=2) -> Workload:
     """16 dense ion tracks x 1e6 deposits, HL 5000 nm, d 2 nm, 100 oversamples,
     log 500 bins over 0.1-1e4 keV/um."""
-    g = torch.Generator(device=device).manual_seed(seed)
-    sizes = torch.full((n_tracks,), n_dep, dtype=torch.long, device=device)
-    part = gen_ion(g, sizes, 5000.0, 5.0, 500.0, device)
+    part = _per_track(device, n_tracks, n_dep, seed,
+                      lambda g, sz: gen_ion(g, sz, 5000.0, 5.0, 500.0, device))
     return _assemble("config1-dense-ion", [part], [n_dep] * n_tracks, 5000.0, 2.0, n_os, seed,
-                     [("log", 500, 0.1, 1e4)], [0] * n_tracks)
+                     [("log", 500, 0.1, 1e4)], [0] * n_tracks, generator=1)
 
 
 def config2_sizes(n_tracks=4096, seed=3, size_scale=1.0, max_size=2_000_000):
@@ -250,17 +276,17 @@ def config2(device="cpu", n_tracks=4096, seed=3, size_scale=1.0, os_scale=1.0,
                     n_os=os_.astype(np.uint32), seed=np.full(nj, seed, dtype=np.uint64),
                     track_id=np.arange(nj, dtype=np.uint64),
                     hists=[("log", 200, 0.01, 1e4)] * nj,
-                    hist_of_job=np.arange(nj, dtype=np.int32))
+                    hist_of_job=np.arange(nj, dtype=np.int32),
+                    generator=np.where(kind, 0, 1).astype(np.int8))
 
 
 def config4(device="cpu", n_tracks=256, n_dep=4_000_000, n_os=1000, seed=5) -> Workload:
     """256 ion tracks x 4e6 deposits (core sigma 3 nm, penumbra to 1000 nm), HL 5000 nm,
     d 10 nm, 1000 oversamples, lin 3000 bins over 0.01-300 keV/um with f(y) and y*f(y)."""
-    g = torch.Generator(device=device).manual_seed(seed)
-    sizes = torch.full((n_tracks,), n_dep, dtype=torch.long, device=device)
-    part = gen_ion(g, sizes, 5000.0, 3.0, 1000.0, device)
+    part = _per_track(device, n_tracks, n_dep, seed,
+                      lambda g, sz: gen_ion(g, sz, 5000.0, 3.0, 1000.0, device))
     return _assemble("config4-large", [part], [n_dep] * n_tracks, 5000.0, 10.0, n_os, seed,
-                     [("lin", 3000, 0.01, 300.0)], [0] * n_tracks)
+                     [("lin", 3000, 0.01, 300.0)], [0] * n_tracks, generator=1)
 
 
 def served_stream(n_jobs=10000, seed=4):
