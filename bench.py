@@ -289,13 +289,16 @@ def cpu_estimate(w, jobs, os_run, secs, wall, threads, kind="port"):
 def cpu_baseline(w, seconds: float, threads: int, seed: int = 0, os_cap=None):
     """Times the oracle on a stratified sample sized for about `seconds` of host time; returns
     (cpu_baseline dict, (jobs, os_run, counts, yfy, stats) of the sample for the parity check)."""
-    full_units = float(w.units)
-    # a first small sample calibrates the rate, the second is sized from it
-    jobs, os_run = stratified_sample(w, min(1.0, 4e6 * threads / full_units), seed, os_cap)
+    n_os = w.n_os.astype(np.int64)
+    full_units = float((w.sizes * (np.minimum(n_os, os_cap) if os_cap else n_os)).sum())
+    # a first small sample calibrates the rate per thread (thread seconds: a small sample keeps
+    # only a few threads busy), the second is sized from it
+    frac0 = min(1.0, 4e6 * threads / full_units)
+    jobs, os_run = stratified_sample(w, frac0, seed, os_cap)
     c, y, js, secs, wall = oracle_sample(w, jobs, os_run, threads)
-    rate = float((w.sizes[jobs] * os_run).sum()) / max(wall, 1e-6)
+    rate = float((w.sizes[jobs] * os_run).sum()) / max(float(secs.sum()), 1e-6) * threads
     frac = min(1.0, rate * seconds / full_units)
-    if frac > 4e6 * threads / full_units:
+    if frac > 1.5 * frac0:
         jobs, os_run = stratified_sample(w, frac, seed, os_cap)
         c, y, js, secs, wall = oracle_sample(w, jobs, os_run, threads)
     return cpu_estimate(w, jobs, os_run, secs, wall, threads), (jobs, os_run, c, y, js)

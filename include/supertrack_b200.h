@@ -165,6 +165,12 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *                      oversamples, 128 or more spheres along an axis) gets window boundary flags
  *                      when more than this many of its deposits are kept; with fewer, its
  *                      spheres fit the shared-memory table without them      (default 16384)
+ *   sort_deposits      prepare blocks (1024 source deposits) that write their kept deposits
+ *                      grouped by d-cell, the groups in the order of their first deposit, so
+ *                      that deposits of one sphere arrive together in the fused kernel: 0 none
+ *                      (source order), 1 the blocks of jobs with window boundary flags (dense
+ *                      multi-window tracks), 2 all. Results do not depend on it (sums are
+ *                      exact)                                                (default 1)
  *   precision          64 = the reference's FP64 arithmetic; 32 = FP32 geometry variant: x, y,
  *                      shifts, the x/y box test, x/y lattice index and sphere distance in float
  *                      (z, keys and energies as in FP64). No reference counterpart: the
@@ -180,7 +186,8 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *                      (captured at the first rerun); 0 = enqueue every call (default 1)
  *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to
  *                      hold every sphere of the batch's largest job); the grid shrinks to fit;
- *                      0 = 30% of free device memory, at most 48 GB          (default 0)
+ *                      0 = 30% of free device memory, or the full grid's tables when they
+ *                      leave 16 GB free; at most 48 GB                       (default 0)
  * st_ctx_get_param also reads "last_grid" (CTAs of the last fused launch), "spill_slots"
  * (slots of each CTA's spill table), "graph_launches" (runs replayed from a CUDA graph) and
  * the host cost of the last launch in microseconds:
@@ -189,8 +196,8 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
 ST_API st_status st_ctx_set_param(st_ctx* ctx, const char* name, int64_t value);
 ST_API st_status st_ctx_get_param(const st_ctx* ctx, const char* name, int64_t* value);
 
-/* Autotuner: picks item_cost, chunk_windows, max_helpers, share_divisor and table_slots for the
- * context's queued jobs by timing them (coordinate descent, at most max_trials batched runs of
+/* Autotuner: picks item_cost, sort_deposits, chunk_windows, max_helpers, share_divisor and
+ * table_slots for the context's queued jobs by timing them (coordinate descent, at most max_trials batched runs of
  * all jobs, best of two each). Replaces the reference's SuggestedCudaBlocks/SuggestedCudaThreads
  * keys (VoxelConstrainedSphereMethod.cu:27-28, Histogram.cu:37-38). Histograms and job states are
  * as before the call;
@@ -200,7 +207,7 @@ typedef struct {
   double best_ms;              /* ... with the chosen parameters                           */
   int64_t item_cost;
   int32_t chunk_windows, max_helpers, share_divisor, table_slots;
-  int32_t trials, reserved;
+  int32_t trials, sort_deposits;
 } st_tune_result;
 ST_API st_status st_ctx_autotune(st_ctx* ctx, int32_t max_trials, st_tune_result* out);
 

@@ -196,11 +196,14 @@ struct st_ctx {
   st::PlanParams cache_plan{};
   int chunk_windows = 4;      // windows (8192 deposits each) per chunk of a shared unit
   int max_helpers = 32;       // helper items per shared unit
-  int64_t spill_budget = 0;   // bytes for the spill tables; 0: 30% of free memory, at most 48 GB
+  int64_t spill_budget = 0;   // bytes for the spill tables; 0: 30% of free memory (or the full
+                              // grid's tables if they leave 16 GB free), at most 48 GB
   int share_divisor = 8;      // shared units: kept > batch units / (share_divisor * grid) ...
   int min_chunks = 4;         // ... and kept > min_chunks chunks
   int precision = 64;         // 32: FP32 geometry variant (x/y geometry in float)
   int64_t flag_min_kept = 16384;  // window flags only for jobs with more kept deposits
+  int sort_deposits = 1;          // prepare blocks that group kept deposits by cell: 0 none,
+                                  // 1 those of window-flagged jobs, 2 all
 
   // results of an enqueued run are copied into pinned buffers and picked up at finish
   JobAux* h_aux = nullptr;
@@ -461,8 +464,15 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     if (c->spill_budget <= 0) cudaMemGetInfo(&free_b, &total_b);
     c->host_meminfo_us = now_us() - tm;
     const size_t have = (size_t)c->gcap * (size_t)c->ggrid * 28;
-    const double budget = c->spill_budget > 0 ? (double)c->spill_budget
-                                              : std::min(0.3 * (double)(free_b + have), 48e9);
+    // default: 30% of free memory, or the whole grid's tables when they still leave 16 GB free
+    // (a batch of huge tracks, whose tables are large, would otherwise run on a fraction of the
+    // SMs); at most 48 GB
+    const double avail = (double)(free_b + have);
+    const double full = (double)gcap * 28.0 * (double)grid;
+    const double budget = c->spill_budget > 0
+                              ? (double)c->spill_budget
+                              : std::min(std::max(0.3 * avail, full <= avail - 16e9 ? full : 0.0),
+                                         48e9);
     const int fit = (int)std::max(1.0, std::floor(budget / ((double)gcap * 28.0)));
     grid = std::min(grid, fit);
   }
@@ -496,6 +506,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.PKEY = (unsigned long long*)c->pkey.p;
   pp.fp32 = c->precision == 32 ? 1 : 0;
   pp.flag_min_kept = c->flag_min_kept;
+  pp.sort = c->sort_deposits;
 
   st::FusedParams& fp = c->cache_fp;
   fp.jobs = pp.jobs;
@@ -1107,6 +1118,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
   else if (n == "precision" && (v == 64 || v == 32)) { c->precision = (int)v; drop_graph(c); }
   else if (n == "flag_min_kept" && v >= 0) c->flag_min_kept = v;
+  else if (n == "sort_deposits" && v >= 0 && v <= 2) c->sort_deposits = (int)v;
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
   else if (n == "pipeline_bytes" && v >= 0) c->pipeline_bytes = v > 0 ? v : ((int64_t)1 << 62);
@@ -1127,6 +1139,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "precision") *v = c->precision;
   else if (n == "flag_min_kept") *v = c->flag_min_kept;
+  else if (n == "sort_deposits") *v = c->sort_deposits;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
   else if (n == "pipeline_bytes") *v = c->pipeline_bytes;
@@ -1183,6 +1196,7 @@ st_status st_ctx_autotune(st_ctx* c, int32_t max_trials, st_tune_result* out) {
   };
   const Knob knobs[] = {
       {"item_cost", {1 << 16, 1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}},
+      {"sort_deposits", {0, 1, 2}},
       {"chunk_windows", {1, 2, 4, 8, 16}},
       {"max_helpers", {8, 16, 32, 64, 148}},
       {"share_divisor", {2, 4, 8, 16, 0}},
@@ -1223,7 +1237,7 @@ st_status st_ctx_autotune(st_ctx* c, int32_t max_trials, st_tune_result* out) {
   out->share_divisor = c->share_divisor;
   out->table_slots = c->table_slots;
   out->trials = trials;
-  out->reserved = 0;
+  out->sort_deposits = c->sort_deposits;
   return ST_OK;
 }
 

@@ -182,6 +182,9 @@ struct PrepareParams {
   int32_t fp32;               // 1: records for the FP32 geometry variant
   int64_t flag_min_kept;      // a flagged job runs with window flags only above this many kept
                               // deposits (fewer spheres than that fit the table without them)
+  int32_t sort;               // prepare blocks that write their kept deposits grouped by cell
+                              // (see k_prep_write): 0 none, 1 those of window-flagged jobs,
+                              // 2 all; the others write them in source order
 };
 
 // Device-side planning of the fused kernel's work items from the kept deposit counts.

@@ -278,6 +278,23 @@ __global__ void __launch_bounds__(1024) k_prep_scan(PrepareParams p) {
   }
 }
 
+// In-block grouping of kept deposits by cell (sorted prepare blocks): a block writes its kept
+// deposits grouped by d-cell (x, y and z after the z-origin shift, each divided by d and rounded
+// down), the groups in the order of their cells' first deposit in the block. Deposits of one cell
+// mostly share a sphere for any shift, so the fused kernel sums them as runs in registers and
+// across lanes instead of one shared-memory insert each; line-ordered tracks keep their order
+// apart from the deposits pulled forward to their cell's first one. Cells are told apart by a
+// kCellHashBins-way hash (a collision only merges two groups). Sort mode 1 groups the blocks of
+// window-flagged jobs (multi-window jobs on fine lattices: the dense tracks whose spheres take
+// several hits that the source order scatters), mode 2 every block.
+constexpr int kCellHashBins = 1024;
+__device__ __forceinline__ unsigned cell_hash_bin(const JobDev& J, double x, double y, double z1) {
+  const unsigned cx = (unsigned)__double2int_rd(st_dmul(x, J.inv_d));
+  const unsigned cy = (unsigned)__double2int_rd(st_dmul(y, J.inv_d));
+  const unsigned cz = (unsigned)__double2int_rd(st_dmul(z1, J.inv_d));
+  return ((cx * 73856093u) ^ (cy * 19349663u) ^ (cz * 83492791u)) & (kCellHashBins - 1);
+}
+
 __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = prep_job(p, b);
@@ -286,8 +303,22 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int kWarpsPerBlock = kPrepThreads / 32;
   constexpr int kRounds = kPrepSlotsPerBlock / kPrepThreads;
+  constexpr int kGroupsPerThread = kPrepSlotsPerBlock / kPrepThreads;
+  constexpr int kHashPerThread = kCellHashBins / kPrepThreads;
   __shared__ int s_warp[kRounds][kWarpsPerBlock];
+  // sorted blocks: the first deposit (block-local index) of every cell-hash bin, and per group
+  // (named by that first deposit) its size, then its offset
+  __shared__ unsigned s_first[kCellHashBins];
+  __shared__ unsigned s_group[kPrepSlotsPerBlock];
+  __shared__ unsigned s_part[kWarpsPerBlock];
   int64_t run = p.blk_offset[b];  // kept index of the next kept deposit of this block
+  const bool sorted = p.sort == 2 || (p.sort == 1 && J.flagged);
+  if (sorted) {
+#pragma unroll
+    for (int t = 0; t < kHashPerThread; ++t) s_first[threadIdx.x * kHashPerThread + t] = ~0u;
+#pragma unroll
+    for (int t = 0; t < kGroupsPerThread; ++t) s_group[threadIdx.x * kGroupsPerThread + t] = 0;
+  }
   const JobAux A = p.aux[j];
   const int E0 = choose_grid_exponent(A.e_min, A.e_max, J.n, A.flags & kAuxNonzero);
   unsigned created_cells = 0;  // cells this thread created (windowed jobs)
@@ -305,6 +336,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
     }
   }
   unsigned keep = 0, m[kRounds];
+  unsigned slot_of[kRounds];  // sorted blocks: cell-hash bin, then group (high 16 bits) and rank
+  if (sorted) __syncthreads();  // tables initialised
 #pragma unroll
   for (int r = 0; r < kRounds; ++r) {
     const int64_t i = i0 + r * kPrepThreads + threadIdx.x;
@@ -314,8 +347,47 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
     m[r] = __ballot_sync(0xffffffffu, k);
     if (lane == 0) s_warp[r][warp] = __popc(m[r]);
     e[r] = k ? J.edep[i] : 0.0;
+    slot_of[r] = 0;
+    if (sorted && k) {
+      slot_of[r] = cell_hash_bin(J, x[r], y[r], z1[r]);
+      atomicMin(&s_first[slot_of[r]], (unsigned)(r * kPrepThreads + threadIdx.x));
+    }
   }
   __syncthreads();
+  if (sorted) {
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      if (keep & (1u << r)) {
+        const unsigned g = s_first[slot_of[r]];
+        slot_of[r] = (g << 16) | atomicAdd(&s_group[g], 1u);
+      }
+    }
+    __syncthreads();
+    // exclusive scan of the group sizes: each thread sums its kGroupsPerThread groups, the warps
+    // scan the thread sums, and the warp totals are scanned in shared memory
+    unsigned v[kGroupsPerThread], tsum = 0;
+#pragma unroll
+    for (int t = 0; t < kGroupsPerThread; ++t) {
+      v[t] = s_group[threadIdx.x * kGroupsPerThread + t];
+      tsum += v[t];
+    }
+    unsigned incl = tsum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) s_part[warp] = incl;
+    __syncthreads();
+    unsigned base = incl - tsum;
+    for (int w = 0; w < warp; ++w) base += s_part[w];
+#pragma unroll
+    for (int t = 0; t < kGroupsPerThread; ++t) {
+      s_group[threadIdx.x * kGroupsPerThread + t] = base;
+      base += v[t];
+    }
+    __syncthreads();
+  }
 #pragma unroll
   for (int r = 0; r < kRounds; ++r) {
     int before = 0, total = 0;
@@ -326,7 +398,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       total += c;
     }
     if (keep & (1u << r)) {
-      const int64_t k = run + before + __popc(m[r] & ((1u << lane) - 1u));
+      // kept index: block order, or the position of the deposit's group and rank in sorted
+      // blocks
+      const int64_t k = sorted ? p.blk_offset[b] + s_group[slot_of[r] >> 16] + (slot_of[r] & 0xFFFFu)
+                               : run + before + __popc(m[r] & ((1u << lane) - 1u));
       const double az = st_dsub(z1[r], J.gSO);
       const double kd = rint(__ddiv_rn(az, J.d));
       const double dz = st_dsub(st_dmul(kd, J.d), az);

@@ -81,7 +81,8 @@ def test_autotune_keeps_state_and_results(work):
 @pytest.mark.parametrize("name,value", [("item_cost", 1 << 16), ("chunk_windows", 1),
                                         ("max_helpers", 8), ("share_divisor", 0),
                                         ("table_slots", 4096), ("flag_min_kept", 0),
-                                        ("flag_min_kept", 1 << 40)])
+                                        ("flag_min_kept", 1 << 40), ("sort_deposits", 0),
+                                        ("sort_deposits", 2)])
 def test_planning_parameters_do_not_change_results(work, name, value):
     res = []
     for set_it in (False, True):
