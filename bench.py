@@ -485,6 +485,16 @@ def serve_leg(dev, batched_value: float, n_jobs: int):
             summ.update({"load": load, "offered": load * batched_value,
                          "arrival_span_s": float(arr[-1] / 1e9)})
             out["loads"].append(summ)
+        # a longer window at 80 % load: the same tracks replayed five times over (50,000 jobs,
+        # each repeat with its own track ids and so its own shifts)
+        wl = serving.repeated(w, 5)
+        arr = serving.poisson_arrivals(wl, 0.8 * batched_value, seed=5)
+        _, _, rec, wall = serving.replay(srv, wl, arr)
+        summ = serving.latency_summary(rec, serving.job_work(wl))
+        summ.update({"load": 0.8, "offered": 0.8 * batched_value, "jobs": wl.n_jobs,
+                     "arrival_span_s": float(arr[-1] / 1e9),
+                     "workload": "the 10,000 jobs replayed five times at 80 % load"})
+        out["long_stream_80pct"] = summ
     out["p99_ms_at_80pct"] = next(l["p99_ms"] for l in out["loads"] if l["load"] == 0.8)
     return out
 

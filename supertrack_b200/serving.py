@@ -6,6 +6,7 @@ This module builds the stream and measures it:
 
 * :func:`served_workload` — the jobs (lognormal sizes, mixed generators, diameters and
   oversample counts, one 200-bin log histogram each), generated on the device;
+* :func:`repeated` — the same jobs several times over (a longer stream on the same tracks);
 * :func:`poisson_arrivals` — arrival times for an offered load in deposit x oversamples per s;
 * :func:`replay` — runs the stream through a server and returns spectra and completion records;
 * :func:`latency_summary` — p50/p95/p99 latency and achieved throughput.
@@ -37,6 +38,22 @@ def served_workload(device="cuda", n_jobs: int = 10000, seed: int = 4, size_scal
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     return w
+
+
+def repeated(w: W.Workload, times: int) -> W.Workload:
+    """w's jobs `times` times over, on the same track tensors: repeat r of job j reads job j's
+    deposits and has track id j + r * n_jobs, so its oversample shifts are its own."""
+    n = w.n_jobs
+    tile = lambda a: np.tile(np.asarray(a), times)
+    r = W.Workload(name=w.name + f"-x{times}", x=w.x, y=w.y, z=w.z, edep=w.edep,
+                   offsets=tile(w.offsets), sizes=tile(w.sizes), half_length=tile(w.half_length),
+                   diameter=tile(w.diameter), n_os=tile(w.n_os), seed=tile(w.seed),
+                   track_id=(tile(w.track_id) + np.repeat(np.arange(times, dtype=np.uint64),
+                                                          n) * np.uint64(n)).astype(np.uint64),
+                   hist_of_job=np.arange(n * times, dtype=np.int32),
+                   hists=list(w.hists) * times, zshift=w.zshift, shift_track=w.shift_track,
+                   generator=None if w.generator is None else tile(w.generator))
+    return r
 
 
 def job_work(w: W.Workload) -> np.ndarray:
