@@ -102,3 +102,22 @@ def test_both_arms_print_the_same_config():
     assert a == b and a["units_per_step"] == w.units
     assert "flushed" in a["l2"]       # a tiny workload fits L2: the GPU arm flushes it
     assert bench.config_dict(2, _sizes_only(), 1, 1.0)["l2"].startswith("inputs larger")
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the CPU restatement, no GPU needed) on the small proton
+    workload prints one JSON line with the contract's keys and the same config as the GPU arm."""
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--config", "0", "--steps", "2", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better",
+              "scaling", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["value"] == line["value"]
+    assert line["config"] == bench.config_dict(0, W.config0(), 1, 1.0)
+    assert len(line["cpu_baseline"]["per_step_values"]) == 2
