@@ -25,7 +25,9 @@ Multi-GPU (torchrun, or --gpus N, which starts its own N ranks): the headline wo
 partitioned across ranks by longest-processing-time first on their deposit*oversamples; each
 rank runs its share as one batched launch, and every step ends with one NCCL all-reduce of the
 spectra (the reference's TH1::Add of the workers' histograms). The total work is fixed (strong
-scaling); value = the workload's units / the slowest rank's time.
+scaling); value = the workload's units / the slowest rank's time. --scaling weak gives every
+rank its own replica of the workload instead (seed offset by 1000 x rank, the same spectrum
+all-reduce); value = all ranks' units / the slowest rank's time.
 
 --impl reference: the reference cannot be built here (CERN ROOT is absent and its histogram
 stage needs device-side cudaDeviceSynchronize, which CUDA 12 rejects), so this arm times the
@@ -93,6 +95,10 @@ def parse(argv=None):
                    help="other configurations measured in the same run (comma list, '' for none)")
     p.add_argument("--scale", type=float, default=1.0,
                    help="track-count scale of the headline workload (1.0 = as specified)")
+    p.add_argument("--scaling", default="strong", choices=["strong", "weak"],
+                   help="several GPUs: strong = the one headline workload LPT-sharded over the "
+                        "ranks; weak = every rank runs its own replica of it (seed offset by "
+                        "1000 x rank)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-fp32", action="store_true",
@@ -123,12 +129,13 @@ DESC = {
 SEED = {0: 1, 1: 2, 2: 3, 4: 5}
 
 
-def make_workload(cfg: int, device, scale: float = 1.0):
+def make_workload(cfg: int, device, scale: float = 1.0, replica: int = 0):
+    """The configuration's workload; replica r > 0 (weak scaling) draws it with seed + 1000 r."""
     import supertrack_b200.workloads as W
     n = {0: 64, 1: 16, 2: 4096, 4: 256}[cfg]
     n = max(1, int(round(n * scale)))
     gen = {0: W.config0, 1: W.config1, 2: W.config2, 4: W.config4}[cfg]
-    return gen(device=device, n_tracks=n, seed=SEED[cfg])
+    return gen(device=device, n_tracks=n, seed=SEED[cfg] + 1000 * replica)
 
 
 L2_BYTES = 126 * 2**20
@@ -139,16 +146,24 @@ def fits_l2(w) -> bool:
     return w.deposits * 88 <= 2 * L2_BYTES
 
 
-def config_dict(cfg: int, w, world: int, scale: float) -> dict:
-    """The workload description both arms print (identical for the same arguments)."""
+def config_dict(cfg: int, w, world: int, scale: float, scaling: str = "strong") -> dict:
+    """The workload description both arms print (identical for the same arguments). Under weak
+    scaling every one of the `world` ranks runs its own replica of w."""
     desc = DESC[cfg] if scale == 1.0 else DESC[cfg] + f" (track count x{scale})"
-    return {"workload": desc, "seed": SEED[cfg], "jobs": w.n_jobs, "deposits": w.deposits,
-            "units_per_step": w.units,
+    reps = world if scaling == "weak" else 1
+    if world == 1:
+        par = "1 GPU"
+    elif scaling == "weak":
+        par = (f"{world} GPUs: one replica of the workload per rank (seed + 1000 x rank), "
+               "one spectrum all-reduce per step")
+    else:
+        par = f"{world} GPUs: LPT job shards, one spectrum all-reduce per step"
+    return {"workload": desc, "seed": SEED[cfg], "jobs": w.n_jobs * reps,
+            "deposits": w.deposits * reps, "units_per_step": w.units * reps,
             "l2": ("L2 flushed before every timed step (a 512 MB write outside the timed events)"
                    if fits_l2(w) else
                    "inputs larger than L2 (tracks + prepared records > 126 MB), no flush"),
-            "parallelism": ("1 GPU" if world == 1 else
-                            f"{world} GPUs: LPT job shards, one spectrum all-reduce per step")}
+            "parallelism": par}
 
 
 def cpu_model() -> str:
@@ -350,9 +365,9 @@ def reference_arm(args, rank, world):
     value = statistics.median([r["value"] for r in res])
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": args.scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": config_dict(args.config, w, world, args.scale),
+            "config": config_dict(args.config, w, world, args.scale, args.scaling),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "cpu_model": cpu_model(), "sample": res[-1]["sample"],
                              "per_step_values": [r["value"] for r in res]},
@@ -505,11 +520,13 @@ def headline(args, rank, world, dev, stream):
     import torch
     import supertrack_b200 as st
     from supertrack_b200.sharding import reduce_spectra_device, shard
-    w = make_workload(args.config, dev, args.scale)
+    weak = world > 1 and args.scaling == "weak"
+    w = make_workload(args.config, dev, args.scale, replica=rank if weak else 0)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()   # the generator's temporaries: the context sizes from free memory
     costs = w.sizes.astype(np.float64) * w.n_os.astype(np.float64)
-    mine = np.array(shard(costs, rank, world) if world > 1 else range(w.n_jobs), dtype=np.int64)
+    mine = np.array(shard(costs, rank, world) if world > 1 and not weak else range(w.n_jobs),
+                    dtype=np.int64)
     ctx = st.Context(dev.index, stream=stream.cuda_stream)
     # every rank holds every histogram of the workload (the same bin layout on all ranks, which
     # the all-reduce needs) and submits its own jobs into theirs
@@ -560,7 +577,7 @@ def headline(args, rank, world, dev, stream):
             launches += n
     clocks = sampler.stop()
     graph_steps = ctx.get_param("graph_launches") - g_before
-    units = w.units
+    units = w.units * (world if weak else 1)   # the whole job's units over all ranks
     value = units * args.steps / (T.ms * 1e-3)
 
     # ---- parity of this run's per-job results against the oracle on the CPU sample (rank 0
@@ -592,9 +609,10 @@ def headline(args, rank, world, dev, stream):
                 ctx2.jobs_reset()
                 ctx2.run("batched")
                 ctx2.read_all_into(out_c.data_ptr(), out_y.data_ptr(), nb)
-        h2d = int(w.sizes[mine].sum()) * 32
+        # bytes of the whole job: every rank uploads its own tracks and reads its spectra back
+        h2d = int(w.deposits) * 32 * (world if weak else 1)
         e2e = {"value": units * e2e_steps / (E.ms * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(nb * 16),
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(nb * 16) * world,
                "steps": e2e_steps}
         ctx2.close()
         del hx
@@ -686,8 +704,8 @@ def headline(args, rank, world, dev, stream):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": T.ms / args.steps, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(args.config, w, world, args.scale),
+        "scaling": args.scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args.config, w, world, args.scale, args.scaling),
         "work_per_step": {"inbox_units": inbox, "hits": hits, "spheres": spheres},
         "gpu_launches": launches,
         "graph_steps": graph_steps,
