@@ -3,10 +3,12 @@
 // HBM layout of one batch:
 //   * input tracks: SoA float64 x, y, z, edep per job (caller memory or the context's arena);
 //   * prepared arena (written once per job, read once per oversample): for every job its kept
-//     deposits (those that can lie inside the voxel for some shift; order preserved) as a padded
-//     run of warp tiles of kWarpTile deposits, stored tile by tile in "lane-blocked" order so a
-//     warp-wide load of row p reads 32 consecutive doubles while lane l owns the kDepPerLane
-//     consecutive deposits l*kDepPerLane .. l*kDepPerLane+kDepPerLane-1 of the tile:
+//     deposits (those that can lie inside the voxel for some shift; in source order, or grouped
+//     by cell inside each prepare block) as a padded run of warp tiles of kWarpTile deposits.
+//     Lane l of a warp tile owns the kDepPerLane consecutive deposits 4l..4l+3 of the tile,
+//     stored "pair-blocked" (prep_slot in vcs_kernels.cu): the pair 4l, 4l+1 at tile slots
+//     2l, 2l+1 and the pair 4l+2, 4l+3 at 64+2l, 64+2l+1, so a warp reads one pair per lane with
+//     one 16-byte load per lane (512 contiguous bytes):
 //       PX, PY  : x, y as loaded (padding slots hold NaN so the box test rejects them)
 //       PDZ2    : (k_z*d - a_z)^2, +inf when the deposit is outside the box in z
 //       PVLO/HI : v = edep / ((2/3) d) on the job's fixed-point grid (128-bit integer)

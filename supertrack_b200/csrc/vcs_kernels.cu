@@ -4,7 +4,7 @@
 //               can be in the voxel for some shift, the z part of the lattice test (k_z and
 //               (k_z*d - a_z)^2, which do not depend on the oversample), the lineal energy
 //               contribution v = edep/((2/3)d), the job's fixed-point exponent range, and the
-//               ordered, lane-blocked compaction of the kept deposits into the prepared arena.
+//               ordered compaction of the kept deposits into the pair-blocked prepared arena.
 //               Follows VoxelConstrainedSphereMethod.cu:138-154 (z shift), :198 (|z| test),
 //               :249-258 (z axis of the membership test), :302/:322 (lineal denominator).
 //   k_fused   : persistent work-stealing kernel over (job, oversample block) items. Per
@@ -50,7 +50,7 @@ constexpr int kGeoBlock = 2;                     // deposits per straight-line g
 //                  strictly inside; |x|, |y| below xy_keep), plus the job's exponent range of
 //                  the contributions v = edep/((2/3)d) over all its deposits;
 //   k_prep_scan  : per job, exclusive scan of its block counts -> block offsets, kept total;
-//   k_prep_write : ordered compaction of the kept deposits into the lane-blocked arena with
+//   k_prep_write : ordered compaction of the kept deposits into the pair-blocked arena with
 //                  the oversample-independent z part of the lattice test;
 //   k_prep_pad   : padding of each job's last warp tile (NaN x so the box test rejects it).
 // A dropped deposit can be inside the box for no shift, so dropping it changes no result.
@@ -68,6 +68,17 @@ __device__ __forceinline__ int find_job(const int64_t* blk_prefix, int n_jobs, i
 // blocks a dozen dependent loads of the binary search before their first track load.
 __device__ __forceinline__ int prep_job(const PrepareParams& p, int64_t b) {
   return p.blk_job ? __ldg(&p.blk_job[b]) - p.job_base : find_job(p.blk_prefix, p.n_jobs, b);
+}
+
+// Slot of kept deposit k of a job in the prepared arena: warp tiles of kWarpTile deposits in
+// which lane l owns deposits 4l..4l+3, stored "pair-blocked": the pair (4l, 4l+1) at tile slots
+// 2l, 2l+1 and the pair (4l+2, 4l+3) at 64 + 2l, 64 + 2l + 1. A warp reads a geometry block
+// (one pair per lane) with one 16-byte load per lane, 512 contiguous bytes per warp.
+__device__ __forceinline__ int64_t prep_slot(const JobDev& J, int64_t k) {
+  const int64_t w = k / kWarpTile;
+  const int rem = (int)(k - w * kWarpTile);
+  const int l = rem / kDepPerLane, pp = rem % kDepPerLane;
+  return J.prep_off + w * kWarpTile + (pp >> 1) * 64 + 2 * l + (pp & 1);
 }
 
 // A windowed job whose kept deposits share cells (fewer than half as many occupied cells as
@@ -405,9 +416,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       const double az = st_dsub(z1[r], J.gSO);
       const double kd = rint(__ddiv_rn(az, J.d));
       const double dz = st_dsub(st_dmul(kd, J.d), az);
-      const int64_t w = k / kWarpTile;
-      const int rem = (int)(k - w * kWarpTile);
-      const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+      const int64_t dst = prep_slot(J, k);
       if (p.fp32) {
         reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__double2float_rn(x[r]), __double2float_rn(y[r]));
         reinterpret_cast<float*>(p.PDZ2)[dst] = __double2float_rn(st_dmul(dz, dz));
@@ -449,9 +458,7 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
   if ((kept % kWarpTile) == 0) return;
   const long long k = kept + threadIdx.x;
   if (k >= (kept / kWarpTile + 1) * kWarpTile) return;
-  const int64_t w = k / kWarpTile;
-  const int rem = (int)(k - w * kWarpTile);
-  const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+  const int64_t dst = prep_slot(J, k);
   if (p.fp32) {
     reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__int_as_float(0x7FC00000), __int_as_float(0x7FC00000));
     reinterpret_cast<float*>(p.PDZ2)[dst] = __int_as_float(0x7F800000);
@@ -480,9 +487,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
   const int cnt = p.blk_count[b];
   for (int q = threadIdx.x; q < cnt; q += kPrepThreads) {
     const int64_t k = k0 + q;
-    const int64_t w = k / kWarpTile;
-    const int rem = (int)(k - w * kWarpTile);
-    const int64_t dst = J.prep_off + w * kWarpTile + (rem % kDepPerLane) * 32 + rem / kDepPerLane;
+    const int64_t dst = prep_slot(J, k);
     double x, y;
     if (p.fp32) {  // float-rounded x, y: the FP32 jobs' cell size covers the rounding
       const float2 xy = reinterpret_cast<const float2*>(p.PX)[dst];
@@ -1033,17 +1038,25 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
     for (int tt = 0; tt < wtiles; ++tt) {
       const int64_t w = wt0 + tt * kWarps + warp;
       if (w < wt_end) {
-        const int64_t tb = J.prep_off + w * kWarpTile + lane;
+        // pair-blocked tile (prep_slot): this lane's deposits p = 0, 1 are the slots tb, tb + 1
+        // and p = 2, 3 the slots tb + 64, tb + 65
+        const int64_t tb = J.prep_off + w * kWarpTile + 2 * lane;
         uint32_t kxv[kDepPerLane], kyv[kDepPerLane];
         unsigned hitmask = 0, boxmask = 0;
         if constexpr (F32) {
           // x' = x + sx, box |x'| < HL', a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a,
           // hit iff (dx^2 + dy^2) + dz^2 <= r^2, every step rounded to float
-          const float2* pxy = reinterpret_cast<const float2*>(P.PX);
-          const float* pdz2 = reinterpret_cast<const float*>(P.PDZ2);
+          const float2* pxy = reinterpret_cast<const float2*>(P.PX) + tb;
+          const float* pdz = reinterpret_cast<const float*>(P.PDZ2) + tb;
+          const float4 xy01 = __ldg(reinterpret_cast<const float4*>(pxy));
+          const float4 xy23 = __ldg(reinterpret_cast<const float4*>(pxy + 64));
+          const float2 dz01 = __ldg(reinterpret_cast<const float2*>(pdz));
+          const float2 dz23 = __ldg(reinterpret_cast<const float2*>(pdz + 64));
   #pragma unroll
           for (int p = 0; p < kDepPerLane; ++p) {
-            const float2 xy = __ldg(&pxy[tb + p * 32]);
+            const float2 xy = p == 0 ? make_float2(xy01.x, xy01.y) : p == 1 ? make_float2(xy01.z, xy01.w)
+                            : p == 2 ? make_float2(xy23.x, xy23.y) : make_float2(xy23.z, xy23.w);
+            const float dzp = p == 0 ? dz01.x : p == 1 ? dz01.y : p == 2 ? dz23.x : dz23.y;
             const float x1 = __fadd_rn(xy.x, sxf);
             const float y1 = __fadd_rn(xy.y, syf);
             const bool inb = fabsf(x1) < J.f_HL && fabsf(y1) < J.f_HL;
@@ -1054,8 +1067,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
             const int iy = __float2int_rn(__fmul_rn(ay, J.f_inv_d));
             const float ddx = __fsub_rn(__fmul_rn((float)ix, J.f_d), ax);
             const float ddy = __fsub_rn(__fmul_rn((float)iy, J.f_d), ay);
-            const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
-                                         __ldg(&pdz2[tb + p * 32]));
+            const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), dzp);
             hitmask |= (unsigned)(inb && dist <= J.f_r2) << p;
             kxv[p] = (uint32_t)ix;
             kyv[p] = (uint32_t)iy;
@@ -1064,12 +1076,15 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
   #pragma unroll
         for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
+          static_assert(kGeoBlock == 2, "a geometry block is one 16-byte load per array");
           double ax[kGeoBlock], ay[kGeoBlock], kdx[kGeoBlock], kdy[kGeoBlock];
           unsigned risk = 0;
+          const double2 xb = __ldg(reinterpret_cast<const double2*>(P.PX + tb + h4 * 32));
+          const double2 yb = __ldg(reinterpret_cast<const double2*>(P.PY + tb + h4 * 32));
   #pragma unroll
           for (int p = 0; p < kGeoBlock; ++p) {
-            const double x1 = st_dadd(__ldg(&P.PX[tb + (h4 + p) * 32]), sx);
-            const double y1 = st_dadd(__ldg(&P.PY[tb + (h4 + p) * 32]), sy);
+            const double x1 = st_dadd(p == 0 ? xb.x : xb.y, sx);
+            const double y1 = st_dadd(p == 0 ? yb.x : yb.y, sy);
             const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
             boxmask |= (unsigned)inb << (h4 + p);
             ax[p] = st_dsub(x1, J.gSO);
@@ -1094,11 +1109,12 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
               }
             }
           }
+          const double2 zb = __ldg(reinterpret_cast<const double2*>(P.PDZ2 + tb + h4 * 32));
   #pragma unroll
           for (int p = 0; p < kGeoBlock; ++p) {
             const double ddx = st_dsub(st_dmul(kdx[p], J.d), ax[p]);
             const double ddy = st_dsub(st_dmul(kdy[p], J.d), ay[p]);
-            const double dz2 = __ldg(&P.PDZ2[tb + (h4 + p) * 32]);
+            const double dz2 = p == 0 ? zb.x : zb.y;
             const double dist = st_dadd(st_dadd(st_dmul(ddx, ddx), st_dmul(ddy, ddy)), dz2);
             const bool hit = ((boxmask >> (h4 + p)) & 1u) && dist <= J.r2;
             hitmask |= (unsigned)hit << (h4 + p);
@@ -1115,7 +1131,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
   #pragma unroll
         for (int p = 0; p < kDepPerLane; ++p) {
           if (hitmask & (1u << p)) {
-            const int64_t idx = tb + p * 32;
+            const int64_t idx = tb + (p >> 1) * 64 + (p & 1);
             const uint64_t lo = __ldg(&P.PVLO[idx]);
             const uint64_t hi = __ldg(&P.PVHI[idx]);
             const uint64_t kzw = __ldg(&P.PKEY[idx]);
