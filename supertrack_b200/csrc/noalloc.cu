@@ -57,7 +57,7 @@ constexpr size_t al(size_t v) { return (v + 255) / 256 * 256; }
 // Byte offsets of every region inside the scratch array.
 struct Layout {
   size_t jobs, aux, hists, blk_prefix, blk_count, blk_off;
-  size_t px, py, pdz2, pvlo, pvhi, pkey, pz;
+  size_t px, py, pdz2, pv, pkey, pz;
   size_t cells;
   size_t gkeys, glo, ghi, gused, gcount, pool;
   size_t items, plan, plan_misc, counter, err, edges, units;
@@ -76,8 +76,7 @@ constexpr Layout make_layout() {
   L.px = o;         o += al(kNaMaxDeposits * 8);
   L.py = o;         o += al(kNaMaxDeposits * 8);
   L.pdz2 = o;       o += al(kNaMaxDeposits * 8);
-  L.pvlo = o;       o += al(kNaMaxDeposits * 8);
-  L.pvhi = o;       o += al(kNaMaxDeposits * 8);
+  L.pv = o;         o += al(kNaMaxDeposits * 16);
   L.pkey = o;       o += al(kNaMaxDeposits * 8);
   L.pz = o;         o += al(kNaMaxDeposits * 8);
   L.cells = o;      o += al((size_t)kNaCellCap * sizeof(st::CellSlot));
@@ -263,8 +262,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   pp.PX = (double*)(base + L.px);
   pp.PY = (double*)(base + L.py);
   pp.PDZ2 = (double*)(base + L.pdz2);
-  pp.PVLO = (unsigned long long*)(base + L.pvlo);
-  pp.PVHI = (unsigned long long*)(base + L.pvhi);
+  pp.PV = (ulonglong2*)(base + L.pv);
   pp.PKEY = (unsigned long long*)(base + L.pkey);
   // the regular path's default: window flags only above this many kept deposits (a track here
   // keeps at most kNaMaxDeposits, so the scratch path never runs windowed, as the regular path
@@ -303,7 +301,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   fp.n_items = q.n_items;
   fp.work_counter = (unsigned int*)(base + L.counter);
   fp.PX = pp.PX; fp.PY = pp.PY; fp.PDZ2 = pp.PDZ2;
-  fp.PVLO = pp.PVLO; fp.PVHI = pp.PVHI; fp.PKEY = pp.PKEY;
+  fp.PV = pp.PV; fp.PKEY = pp.PKEY;
   fp.gkeys = (uint64_t*)(base + L.gkeys);
   fp.glo = (unsigned long long*)(base + L.glo);
   fp.ghi = (unsigned long long*)(base + L.ghi);

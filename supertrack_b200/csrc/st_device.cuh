@@ -11,7 +11,8 @@
 //     one 16-byte load per lane (512 contiguous bytes):
 //       PX, PY  : x, y as loaded (padding slots hold NaN so the box test rejects them)
 //       PDZ2    : (k_z*d - a_z)^2, +inf when the deposit is outside the box in z
-//       PVLO/HI : v = edep / ((2/3) d) on the job's fixed-point grid (128-bit integer)
+//       PV      : v = edep / ((2/3) d) on the job's fixed-point grid, a 128-bit integer stored
+//                 as one 16-byte {low, high} record (one vector load per hit)
 //       PKEY    : k_z * N*N (the z part of the sphere key); bit 63 flags boundary deposits
 //   * spill tables: one open-addressing table per resident CTA for spheres that do not fit
 //     the CTA's shared-memory table (keys, 128-bit accumulators, used-slot list);
@@ -125,8 +126,7 @@ struct FusedParams {
   const double* PX;
   const double* PY;
   const double* PDZ2;
-  const unsigned long long* PVLO;  // contribution on the job's grid, low 64 bits
-  const unsigned long long* PVHI;  // high 64 bits
+  const ulonglong2* PV;            // contribution on the job's grid: {low, high} 64-bit words
   const unsigned long long* PKEY;  // k_z * N*N, bit 63 = boundary deposit
   // spill tables: gridDim.x tables of gcap slots each
   uint64_t* gkeys;
@@ -178,8 +178,7 @@ struct PrepareParams {
   double* PX;                 // FP32 variant: float2 {x, y} per slot
   double* PY;                 // FP32 variant: unused
   double* PDZ2;               // FP32 variant: float dz^2 at the slot's float index
-  unsigned long long* PVLO;
-  unsigned long long* PVHI;
+  ulonglong2* PV;
   unsigned long long* PKEY;
   int32_t fp32;               // 1: records for the FP32 geometry variant
   int64_t flag_min_kept;      // a flagged job runs with window flags only above this many kept

@@ -427,8 +427,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       }
       uint64_t lo, hi;
       to_fixed(__ddiv_rn(e[r], J.denom), E0, &lo, &hi);
-      p.PVLO[dst] = lo;
-      p.PVHI[dst] = hi;
+      p.PV[dst] = make_ulonglong2(lo, hi);
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (A.windowed) {
         p.PZ[dst] = z1[r];
@@ -467,8 +466,7 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
     p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
     p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
   }
-  p.PVLO[dst] = 0;
-  p.PVHI[dst] = 0;
+  p.PV[dst] = make_ulonglong2(0, 0);
   p.PKEY[dst] = 0;
 }
 
@@ -1132,8 +1130,9 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         for (int p = 0; p < kDepPerLane; ++p) {
           if (hitmask & (1u << p)) {
             const int64_t idx = tb + (p >> 1) * 64 + (p & 1);
-            const uint64_t lo = __ldg(&P.PVLO[idx]);
-            const uint64_t hi = __ldg(&P.PVHI[idx]);
+            const ulonglong2 v = __ldg(&P.PV[idx]);
+            const uint64_t lo = v.x;
+            const uint64_t hi = v.y;
             const uint64_t kzw = __ldg(&P.PKEY[idx]);
             // (the FP32 form converts a lattice index like the reference's llrint: sign-extended)
             const uint64_t key =
