@@ -138,7 +138,7 @@ struct st_ctx {
   std::vector<JobHost> jobs;
 
   DevBuf track_arena;
-  DevBuf px, py, pdz2, pv, pkey;
+  DevBuf pxy, pdz2, pv, pkey;
   DevBuf d_jobs, d_aux, d_hists, d_items, d_blk, d_counter, d_err, d_blk_count, d_blk_off, d_blk_job;
   DevBuf c_cells, pz;               // cell arena and shifted z of flagged jobs
   DevBuf u_next, u_done, u_table, pool;  // shared units and the spill-table pool
@@ -302,8 +302,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
       arena_total += J.track.n;
     }
   }
-  ST_CUDA(ensure(c->px, prep_total * 8), "prepared arena");
-  ST_CUDA(ensure(c->py, prep_total * 8), "prepared arena");
+  ST_CUDA(ensure(c->pxy, prep_total * 16), "prepared arena");
+
   ST_CUDA(ensure(c->pdz2, prep_total * 8), "prepared arena");
   ST_CUDA(ensure(c->pv, prep_total * 16), "prepared arena");
   ST_CUDA(ensure(c->pkey, prep_total * 8), "prepared arena");
@@ -497,8 +497,8 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   pp.blk_offset = (int64_t*)c->d_blk_off.p;
   pp.cells = (st::CellSlot*)c->c_cells.p;
   pp.PZ = (double*)c->pz.p;
-  pp.PX = (double*)c->px.p;
-  pp.PY = (double*)c->py.p;
+  pp.PXY = (double2*)c->pxy.p;
+
   pp.PDZ2 = (double*)c->pdz2.p;
   pp.PV = (ulonglong2*)c->pv.p;
   pp.PKEY = (unsigned long long*)c->pkey.p;
@@ -514,7 +514,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   fp.n_items = (const int*)((char*)c->d_plan_misc.p + 8);
   fp.flush_threshold = 1024;
   fp.work_counter = (unsigned int*)c->d_counter.p;
-  fp.PX = pp.PX; fp.PY = pp.PY; fp.PDZ2 = pp.PDZ2;
+  fp.PXY = pp.PXY; fp.PDZ2 = pp.PDZ2;
   fp.PV = pp.PV; fp.PKEY = pp.PKEY;
   fp.gkeys = (uint64_t*)c->g_keys.p;
   fp.glo = (unsigned long long*)c->g_lo.p;
@@ -1033,7 +1033,7 @@ st_status st_ctx_destroy(st_ctx* c) {
   if (!c) return ST_ERR_INVALID_ARGUMENT;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->track_arena, &c->px, &c->py, &c->pdz2, &c->pv, &c->pkey,
+  DevBuf* bufs[] = {&c->track_arena, &c->pxy, &c->pdz2, &c->pv, &c->pkey,
                     &c->d_jobs, &c->d_aux, &c->d_hists, &c->d_items, &c->d_blk,
                     &c->d_counter, &c->d_err, &c->d_blk_count, &c->d_blk_off, &c->d_blk_job, &c->c_cells,
                     &c->pz, &c->u_next, &c->u_done, &c->u_table,

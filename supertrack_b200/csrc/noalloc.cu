@@ -57,7 +57,7 @@ constexpr size_t al(size_t v) { return (v + 255) / 256 * 256; }
 // Byte offsets of every region inside the scratch array.
 struct Layout {
   size_t jobs, aux, hists, blk_prefix, blk_count, blk_off;
-  size_t px, py, pdz2, pv, pkey, pz;
+  size_t pxy, pdz2, pv, pkey, pz;
   size_t cells;
   size_t gkeys, glo, ghi, gused, gcount, pool;
   size_t items, plan, plan_misc, counter, err, edges, units;
@@ -73,8 +73,8 @@ constexpr Layout make_layout() {
   L.blk_prefix = o; o += al(2 * 8);
   L.blk_count = o;  o += al(kNaBlocks * 4);
   L.blk_off = o;    o += al(kNaBlocks * 8);
-  L.px = o;         o += al(kNaMaxDeposits * 8);
-  L.py = o;         o += al(kNaMaxDeposits * 8);
+  L.pxy = o;        o += al(kNaMaxDeposits * 16);
+
   L.pdz2 = o;       o += al(kNaMaxDeposits * 8);
   L.pv = o;         o += al(kNaMaxDeposits * 16);
   L.pkey = o;       o += al(kNaMaxDeposits * 8);
@@ -259,8 +259,8 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   pp.cells = (st::CellSlot*)(base + L.cells);
   pp.blk_base = 0;
   pp.PZ = (double*)(base + L.pz);
-  pp.PX = (double*)(base + L.px);
-  pp.PY = (double*)(base + L.py);
+  pp.PXY = (double2*)(base + L.pxy);
+
   pp.PDZ2 = (double*)(base + L.pdz2);
   pp.PV = (ulonglong2*)(base + L.pv);
   pp.PKEY = (unsigned long long*)(base + L.pkey);
@@ -300,7 +300,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   fp.items = q.items;
   fp.n_items = q.n_items;
   fp.work_counter = (unsigned int*)(base + L.counter);
-  fp.PX = pp.PX; fp.PY = pp.PY; fp.PDZ2 = pp.PDZ2;
+  fp.PXY = pp.PXY; fp.PDZ2 = pp.PDZ2;
   fp.PV = pp.PV; fp.PKEY = pp.PKEY;
   fp.gkeys = (uint64_t*)(base + L.gkeys);
   fp.glo = (unsigned long long*)(base + L.glo);

@@ -9,7 +9,8 @@
 //     stored "pair-blocked" (prep_slot in vcs_kernels.cu): the pair 4l, 4l+1 at tile slots
 //     2l, 2l+1 and the pair 4l+2, 4l+3 at 64+2l, 64+2l+1, so a warp reads one pair per lane with
 //     one 16-byte load per lane (512 contiguous bytes):
-//       PX, PY  : x, y as loaded (padding slots hold NaN so the box test rejects them)
+//       PXY     : {x, y} as loaded, one 16-byte record per slot (padding slots hold NaN so the
+//                 box test rejects them); a lane's pair of slots is one 32-byte load
 //       PDZ2    : (k_z*d - a_z)^2, +inf when the deposit is outside the box in z
 //       PV      : v = edep / ((2/3) d) on the job's fixed-point grid, a 128-bit integer stored
 //                 as one 16-byte {low, high} record (one vector load per hit)
@@ -123,8 +124,7 @@ struct FusedParams {
   const int* n_items;         // written by the planner
   int32_t flush_threshold;    // smem table occupancy that triggers a flush to the spill table
   unsigned int* work_counter; // next item to claim
-  const double* PX;
-  const double* PY;
+  const double2* PXY;         // {x, y} per slot (FP32 variant: float2 {x, y} at the slot's index)
   const double* PDZ2;
   const ulonglong2* PV;            // contribution on the job's grid: {low, high} 64-bit words
   const unsigned long long* PKEY;  // k_z * N*N, bit 63 = boundary deposit
@@ -175,8 +175,7 @@ struct PrepareParams {
   int64_t* blk_offset;        // first kept index of each prepare block inside its job
   CellSlot* cells;            // cell arena (flagged jobs)
   double* PZ;                 // z after the z-origin shift (flagged jobs only)
-  double* PX;                 // FP32 variant: float2 {x, y} per slot
-  double* PY;                 // FP32 variant: unused
+  double2* PXY;               // {x, y} per slot; FP32 variant: float2 {x, y} at the slot's index
   double* PDZ2;               // FP32 variant: float dz^2 at the slot's float index
   ulonglong2* PV;
   unsigned long long* PKEY;

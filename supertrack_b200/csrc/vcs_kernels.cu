@@ -418,11 +418,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
       const double dz = st_dsub(st_dmul(kd, J.d), az);
       const int64_t dst = prep_slot(J, k);
       if (p.fp32) {
-        reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__double2float_rn(x[r]), __double2float_rn(y[r]));
+        reinterpret_cast<float2*>(p.PXY)[dst] = make_float2(__double2float_rn(x[r]), __double2float_rn(y[r]));
         reinterpret_cast<float*>(p.PDZ2)[dst] = __double2float_rn(st_dmul(dz, dz));
       } else {
-        p.PX[dst] = x[r];
-        p.PY[dst] = y[r];
+        p.PXY[dst] = make_double2(x[r], y[r]);
         p.PDZ2[dst] = st_dmul(dz, dz);
       }
       uint64_t lo, hi;
@@ -459,11 +458,11 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
   if (k >= (kept / kWarpTile + 1) * kWarpTile) return;
   const int64_t dst = prep_slot(J, k);
   if (p.fp32) {
-    reinterpret_cast<float2*>(p.PX)[dst] = make_float2(__int_as_float(0x7FC00000), __int_as_float(0x7FC00000));
+    reinterpret_cast<float2*>(p.PXY)[dst] = make_float2(__int_as_float(0x7FC00000), __int_as_float(0x7FC00000));
     reinterpret_cast<float*>(p.PDZ2)[dst] = __int_as_float(0x7F800000);
   } else {
-    p.PX[dst] = __longlong_as_double(0x7FF8000000000000ll);
-    p.PY[dst] = __longlong_as_double(0x7FF8000000000000ll);
+    p.PXY[dst] = make_double2(__longlong_as_double(0x7FF8000000000000ll),
+                              __longlong_as_double(0x7FF8000000000000ll));
     p.PDZ2[dst] = __longlong_as_double(0x7FF0000000000000ll);
   }
   p.PV[dst] = make_ulonglong2(0, 0);
@@ -488,12 +487,13 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
     const int64_t dst = prep_slot(J, k);
     double x, y;
     if (p.fp32) {  // float-rounded x, y: the FP32 jobs' cell size covers the rounding
-      const float2 xy = reinterpret_cast<const float2*>(p.PX)[dst];
+      const float2 xy = reinterpret_cast<const float2*>(p.PXY)[dst];
       x = xy.x;
       y = xy.y;
     } else {
-      x = p.PX[dst];
-      y = p.PY[dst];
+      const double2 xy = p.PXY[dst];
+      x = xy.x;
+      y = xy.y;
     }
     const double z = p.PZ[dst];
     const uint32_t win = (uint32_t)(k / kWindow);
@@ -544,6 +544,14 @@ __device__ __forceinline__ bool gtable_add(uint64_t* gk, unsigned long long* glo
     h = (h + 1) & mask;
   }
   return false;
+}
+
+// {x, y} of two consecutive slots (32 bytes, 32-byte aligned: a lane's pair in a pair-blocked
+// tile) with one 256-bit read-only load.
+__device__ __forceinline__ void ldg_xy_pair(const double2* p, double* v) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(p));
 }
 
 // Dynamic shared memory of the fused kernel. The sphere table sits at fixed offsets (so that its
@@ -1044,7 +1052,7 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         if constexpr (F32) {
           // x' = x + sx, box |x'| < HL', a = x' - gSO, k = rint(a * (1/d)), dx = k*d - a,
           // hit iff (dx^2 + dy^2) + dz^2 <= r^2, every step rounded to float
-          const float2* pxy = reinterpret_cast<const float2*>(P.PX) + tb;
+          const float2* pxy = reinterpret_cast<const float2*>(P.PXY) + tb;
           const float* pdz = reinterpret_cast<const float*>(P.PDZ2) + tb;
           const float4 xy01 = __ldg(reinterpret_cast<const float4*>(pxy));
           const float4 xy23 = __ldg(reinterpret_cast<const float4*>(pxy + 64));
@@ -1074,15 +1082,15 @@ __device__ __forceinline__ void superimpose(const FusedParams& P, const FusedJob
         // geometry in straight-line blocks of kGeoBlock deposits, so their FP64 chains interleave
   #pragma unroll
         for (int h4 = 0; h4 < kDepPerLane; h4 += kGeoBlock) {
-          static_assert(kGeoBlock == 2, "a geometry block is one 16-byte load per array");
+          static_assert(kGeoBlock == 2, "a geometry block is a lane's pair of slots");
           double ax[kGeoBlock], ay[kGeoBlock], kdx[kGeoBlock], kdy[kGeoBlock];
           unsigned risk = 0;
-          const double2 xb = __ldg(reinterpret_cast<const double2*>(P.PX + tb + h4 * 32));
-          const double2 yb = __ldg(reinterpret_cast<const double2*>(P.PY + tb + h4 * 32));
+          double xy[4];  // x0, y0, x1, y1 of the pair: one 32-byte load
+          ldg_xy_pair(P.PXY + tb + h4 * 32, xy);
   #pragma unroll
           for (int p = 0; p < kGeoBlock; ++p) {
-            const double x1 = st_dadd(p == 0 ? xb.x : xb.y, sx);
-            const double y1 = st_dadd(p == 0 ? yb.x : yb.y, sy);
+            const double x1 = st_dadd(xy[2 * p], sx);
+            const double y1 = st_dadd(xy[2 * p + 1], sy);
             const bool inb = fabs(x1) < J.HL && fabs(y1) < J.HL;
             boxmask |= (unsigned)inb << (h4 + p);
             ax[p] = st_dsub(x1, J.gSO);
