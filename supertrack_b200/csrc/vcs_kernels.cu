@@ -306,7 +306,9 @@ __device__ __forceinline__ unsigned cell_hash_bin(const JobDev& J, double x, dou
   return ((cx * 73856093u) ^ (cy * 19349663u) ^ (cz * 83492791u)) & (kCellHashBins - 1);
 }
 
-__global__ void __launch_bounds__(kPrepThreads) k_prep_write(PrepareParams p) {
+// Four blocks per SM (64 registers, a few bytes of spills): the stage is memory-bound, and the
+// fourth block's loads in flight are worth more than the spills cost.
+__global__ void __launch_bounds__(kPrepThreads, 4) k_prep_write(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
