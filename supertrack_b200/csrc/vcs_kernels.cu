@@ -187,7 +187,8 @@ __device__ __forceinline__ bool cells_foreign(const PrepareParams& p, const JobD
   return foreign;
 }
 
-__global__ void __launch_bounds__(kPrepThreads) k_prep_count(PrepareParams p) {
+// Eight blocks per SM (32 registers): more track loads in flight.
+__global__ void __launch_bounds__(kPrepThreads, 8) k_prep_count(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
@@ -475,7 +476,8 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
 // the 27 cells around it holds a deposit of another window. A sphere whose hits in a window are
 // all non-boundary has no hit in any other window (its hits are within distance d of each other),
 // so the fused kernel can bin it as soon as the window is done.
-__global__ void __launch_bounds__(kPrepThreads) k_prep_flag(PrepareParams p) {
+// Eight blocks per SM (32 registers): the cell probes are L2 latency, which more warps hide.
+__global__ void __launch_bounds__(kPrepThreads, 8) k_prep_flag(PrepareParams p) {
   const int64_t b = p.blk_base + blockIdx.x;
   const int j = prep_job(p, b);
   const JobDev J = p.jobs[j];
