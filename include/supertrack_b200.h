@@ -165,6 +165,12 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *                      oversamples, 128 or more spheres along an axis) gets window boundary flags
  *                      when more than this many of its deposits are kept; with fewer, its
  *                      spheres fit the shared-memory table without them      (default 16384)
+ *   flag_cells_limit   boundary flags of such a job are found in a hash of cells of side d (27
+ *                      cells probed per kept deposit) or of side 2d (8 probed; more deposits come
+ *                      out flagged, whose spheres are then summed through the spill log at every
+ *                      oversample): side 2d when its deposits per sphere diameter of track
+ *                      length, n * d / (2 HL), times its oversamples are at most this; 0 = side
+ *                      d for every job. Results do not depend on it          (default 25000)
  *   sort_deposits      prepare blocks (1024 source deposits) that write their kept deposits
  *                      grouped by d-cell, the groups in the order of their first deposit, so
  *                      that deposits of one sphere arrive together in the fused kernel: 0 none
@@ -196,8 +202,8 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
 ST_API st_status st_ctx_set_param(st_ctx* ctx, const char* name, int64_t value);
 ST_API st_status st_ctx_get_param(const st_ctx* ctx, const char* name, int64_t* value);
 
-/* Autotuner: picks item_cost, sort_deposits, chunk_windows, max_helpers, share_divisor and
- * table_slots for the context's queued jobs by timing them (coordinate descent, at most max_trials batched runs of
+/* Autotuner: picks item_cost, sort_deposits, chunk_windows, max_helpers, share_divisor,
+ * table_slots and flag_cells_limit for the context's queued jobs by timing them (coordinate descent, at most max_trials batched runs of
  * all jobs, best of two each). Replaces the reference's SuggestedCudaBlocks/SuggestedCudaThreads
  * keys (VoxelConstrainedSphereMethod.cu:27-28, Histogram.cu:37-38). Histograms and job states are
  * as before the call;
@@ -208,6 +214,7 @@ typedef struct {
   int64_t item_cost;
   int32_t chunk_windows, max_helpers, share_divisor, table_slots;
   int32_t trials, sort_deposits;
+  int64_t flag_cells_limit;
 } st_tune_result;
 ST_API st_status st_ctx_autotune(st_ctx* ctx, int32_t max_trials, st_tune_result* out);
 

@@ -280,7 +280,7 @@ class Context:
         (st_ctx_autotune); histograms and job states are unchanged."""
         r = _capi.st_tune_result()
         self._check(lib().st_ctx_autotune(self._h, max_trials, C.byref(r)), "st_ctx_autotune")
-        return {f: getattr(r, f) for f, _ in _capi.st_tune_result._fields_ if f != "reserved"}
+        return {f: getattr(r, f) for f, _ in _capi.st_tune_result._fields_}
 
     def histogram(self, kind: str, nbins: int, lower: float, upper: float) -> int:
         hid = C.c_int32(-1)

@@ -76,7 +76,7 @@ class st_tune_result(C.Structure):
     _fields_ = [("default_ms", C.c_double), ("best_ms", C.c_double), ("item_cost", C.c_int64),
                 ("chunk_windows", C.c_int32), ("max_helpers", C.c_int32),
                 ("share_divisor", C.c_int32), ("table_slots", C.c_int32), ("trials", C.c_int32),
-                ("sort_deposits", C.c_int32)]
+                ("sort_deposits", C.c_int32), ("flag_cells_limit", C.c_int64)]
 
 
 class st_run_info(C.Structure):

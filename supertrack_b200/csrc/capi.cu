@@ -202,6 +202,7 @@ struct st_ctx {
   int min_chunks = 4;         // ... and kept > min_chunks chunks
   int precision = 64;         // 32: FP32 geometry variant (x/y geometry in float)
   int64_t flag_min_kept = 16384;  // window flags only for jobs with more kept deposits
+  int64_t flag_cells_limit = st::kFlagCellsLimit;  // flag cells of side 2d up to this density*OS
   int sort_deposits = 1;          // prepare blocks that group kept deposits by cell: 0 none,
                                   // 1 those of window-flagged jobs, 2 all
 
@@ -356,16 +357,20 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
                  D.N >= 128 && D.N < (1u << (st::kCellBits - 2))) ? 1 : 0;
     D.cell_cap = 0;
     D.cell_off = 0;
-    // two hits of one sphere are within d of each other; in the FP32 form within d plus a few
-    // float roundings of coordinates below 4HL' (HL' 2^-16 covers them)
-    D.cell_size = J.g.sphereDiameter * (1.0 + 0x1p-10) +
-                  (f32 ? J.g.scoringRegionHalfLength * 0x1p-16 : 0.0);
+    // flag cells: two hits of one sphere are within d of each other; in the FP32 form within d
+    // plus a few float roundings of coordinates below 4HL' (HL' 2^-16 covers them). Side twice
+    // that for tracks with few deposits per d of track length times oversamples.
+    const double per_d = (double)J.track.n * J.g.sphereDiameter /
+                         (2.0 * J.g.scoringRegionHalfLength);
+    D.cell_nbr8 = (D.flagged && per_d * J.desc.n_oversamples <= (double)c->flag_cells_limit) ? 1 : 0;
+    D.cell_size = (D.cell_nbr8 ? 2.0 : 1.0) *
+                  (J.g.sphereDiameter * (1.0 + 0x1p-10) +
+                   (f32 ? J.g.scoringRegionHalfLength * 0x1p-16 : 0.0));
     D.f_HL = (float)J.g.scoringRegionHalfLength;
     D.f_gSO = (float)J.g.greatestSphereOffset;
     D.f_d = (float)J.g.sphereDiameter;
     D.f_inv_d = 1.0f / D.f_d;
     D.f_r2 = (float)D.r2;
-    D.f_pad = 0.0f;
     if (D.flagged) {
       D.cell_cap = next_pow2((uint64_t)2 * (uint64_t)J.track.n);
       D.cell_off = cells_total;
@@ -1116,6 +1121,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "shared_min_chunks" && v >= 1 && v <= 1 << 20) c->min_chunks = (int)v;
   else if (n == "precision" && (v == 64 || v == 32)) { c->precision = (int)v; drop_graph(c); }
   else if (n == "flag_min_kept" && v >= 0) c->flag_min_kept = v;
+  else if (n == "flag_cells_limit" && v >= 0) c->flag_cells_limit = v;
   else if (n == "sort_deposits" && v >= 0 && v <= 2) c->sort_deposits = (int)v;
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
@@ -1137,6 +1143,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "shared_min_chunks") *v = c->min_chunks;
   else if (n == "precision") *v = c->precision;
   else if (n == "flag_min_kept") *v = c->flag_min_kept;
+  else if (n == "flag_cells_limit") *v = c->flag_cells_limit;
   else if (n == "sort_deposits") *v = c->sort_deposits;
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
@@ -1199,6 +1206,7 @@ st_status st_ctx_autotune(st_ctx* c, int32_t max_trials, st_tune_result* out) {
       {"max_helpers", {8, 16, 32, 64, 148}},
       {"share_divisor", {2, 4, 8, 16, 0}},
       {"table_slots", {0, 4096}},
+      {"flag_cells_limit", {0, st::kFlagCellsLimit, (int64_t)1 << 50}},
   };
   out->default_ms = trial();
   double best = out->default_ms;
@@ -1236,6 +1244,7 @@ st_status st_ctx_autotune(st_ctx* c, int32_t max_trials, st_tune_result* out) {
   out->table_slots = c->table_slots;
   out->trials = trials;
   out->sort_deposits = c->sort_deposits;
+  out->flag_cells_limit = c->flag_cells_limit;
   return ST_OK;
 }
 

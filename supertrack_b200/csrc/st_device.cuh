@@ -53,7 +53,8 @@ struct JobDev {
   int32_t shift_track;
   int32_t hist;       // histogram index
   // boundary flags (see k_prep_flag): computed when `flagged`; the cell hash of the job lives in
-  // the cell arena at [cell_off, cell_off + cell_cap)
+  // the cell arena at [cell_off, cell_off + cell_cap); its cells have a side slightly above d (27
+  // neighbour cells probed per deposit) or, with cell_nbr8, slightly above 2d (eight probed)
   int32_t flagged;
   uint32_t cell_cap;
   int64_t cell_off;
@@ -64,7 +65,7 @@ struct JobDev {
   float f_d;
   float f_inv_d;
   float f_r2;
-  float f_pad;
+  int32_t cell_nbr8;
 };
 
 // Deposits of a windowed job are processed in windows of consecutive kept deposits: kWindow (two
@@ -223,6 +224,11 @@ constexpr int kCtaTile = kFusedWarps * kWarpTile;    // kept deposits of one war
 constexpr int kWinTiles = 2;                          // warp tiles per warp in a window
 constexpr int kCoarseTiles = 4;                       // ... in a coarse window (dense spheres)
 constexpr int kWindow = kWinTiles * kCtaTile;         // kept deposits per window (8192)
+// A flagged job uses flag cells of side 2d (eight probes per deposit instead of 27, but more
+// deposits flagged, whose spheres then pass through the spill log at every oversample) when its
+// deposits per sphere diameter of track length, n * d / (2 HL), times its oversamples are at most
+// this (context parameter flag_cells_limit).
+constexpr int64_t kFlagCellsLimit = 25000;
 constexpr int kCellBits = 21;                         // bits per axis of a cell key
 
 }  // namespace st

@@ -81,12 +81,12 @@ __device__ __forceinline__ int64_t prep_slot(const JobDev& J, int64_t k) {
   return J.prep_off + w * kWarpTile + (pp >> 1) * 64 + 2 * l + (pp & 1);
 }
 
-// A windowed job whose kept deposits share cells (fewer than half as many occupied cells as
-// deposits: several hits per sphere) runs with coarse windows of kCoarseTiles warp tiles per
-// warp; others with kWinTiles. Its cells record windows of kWindow deposits, a coarse window is
-// two of them.
-__device__ __forceinline__ bool coarse_windows(const JobAux& A) {
-  return A.windowed && 2 * (long long)A.cells < A.kept;
+// A windowed job whose kept deposits share cells (fewer than half as many occupied flag cells
+// of side d as deposits, or a quarter as many of side 2d: several hits per sphere) runs with
+// coarse windows of kCoarseTiles warp tiles per warp; others with kWinTiles. Its cells record
+// windows of kWindow deposits, a coarse window is two of them.
+__device__ __forceinline__ bool coarse_windows(const JobDev& J, const JobAux& A) {
+  return A.windowed && (J.cell_nbr8 ? 4 : 2) * (long long)A.cells < A.kept;
 }
 
 __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y, double z) {
@@ -94,9 +94,15 @@ __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y
   return fabs(z1) < J.HL && fabs(x) < J.xy_keep && fabs(y) < J.xy_keep;
 }
 
-// Cell of side cell_size (slightly above d) containing (x, y, z): integer cell coordinates,
-// offset to be non-negative. Two deposits within distance d of each other lie in the same or in
-// adjacent cells.
+// Flag cell of side cell_size containing (x, y, z): integer cell coordinates, offset to be
+// non-negative. A job's flag cells have a side slightly above d or slightly above 2d
+// (JobDev::cell_nbr8). With side d, two deposits within distance d of each other lie in the same
+// or in adjacent cells: 27 cells around a point hold every deposit within d of it. With side 2d,
+// a deposit within d of a point lies in the point's cell or in the neighbour cell on the side of
+// the half of the cell the point is in: per axis, with u the point's coordinate over the side,
+// |u' - u| < 1/2 - 2^-12 for the other deposit's u', so floor(u') is floor(u) - 1 or floor(u)
+// when u - floor(u) < 1/2, and floor(u) or floor(u) + 1 otherwise (the quotients' rounding
+// errors are far below the margin): eight cells hold every deposit within d.
 struct CellCoord {
   long long x, y, z;
 };
@@ -105,6 +111,24 @@ __device__ __forceinline__ CellCoord cell_of(double x, double y, double z, doubl
   const long long off = 1ll << (kCellBits - 1);
   return {(long long)floor(__ddiv_rn(x, cs)) + off, (long long)floor(__ddiv_rn(y, cs)) + off,
           (long long)floor(__ddiv_rn(z, cs)) + off};
+}
+
+// The cell of a point (as cell_of) and, per axis, the side of its neighbour cells (-1: the point
+// is in the lower half of its cell).
+struct CellNbr {
+  CellCoord c;
+  int sx, sy, sz;
+};
+
+__device__ __forceinline__ int half_side(double u) {
+  return st_dsub(u, floor(u)) < 0.5 ? -1 : 1;
+}
+
+__device__ __forceinline__ CellNbr cell_nbr(double x, double y, double z, double cs) {
+  const long long off = 1ll << (kCellBits - 1);
+  const double u = __ddiv_rn(x, cs), v = __ddiv_rn(y, cs), w = __ddiv_rn(z, cs);
+  return {{(long long)floor(u) + off, (long long)floor(v) + off, (long long)floor(w) + off},
+          half_side(u), half_side(v), half_side(w)};
 }
 
 // Key of the cell at offset (dx, dy, dz) from c.
@@ -144,29 +168,38 @@ __device__ __forceinline__ bool slot_foreign(const ulonglong2& v, uint32_t win, 
          (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
 }
 
-// True when one of the neighbour cells c0 .. c0 + kFlagBatch - 1 (of the 27 around cc) holds a
-// deposit of another window. Their first hash slots are loaded together, so a lane has three
-// L2 round trips in flight instead of one; a cell whose first slot holds another key continues
+// Key of neighbour cell c (0..26) of the 27 around a side-d cell, or (0..7) of the eight around
+// a point in a side-2d cell: offset n.sx on x when bit 0 of c is set, n.sy on y for bit 1, n.sz
+// on z for bit 2.
+__device__ __forceinline__ uint64_t nbr_key27(const CellCoord& cc, int c) {
+  return cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1);
+}
+__device__ __forceinline__ uint64_t nbr_key8(const CellNbr& n, int c) {
+  return cell_key(n.c, (c & 1) ? n.sx : 0, (c & 2) ? n.sy : 0, (c & 4) ? n.sz : 0);
+}
+
+// True when one of the neighbour cells c0 .. c0 + BATCH - 1 (keys from key_of) holds a deposit
+// of another window. Their first hash slots are loaded together, so a lane has several L2
+// round trips in flight instead of one; a cell whose first slot holds another key continues
 // probing alone. The hash is read-only here (k_prep_write filled it), and the neighbourhoods of
 // a block's deposits overlap, so cached loads serve many probes from L1.
-constexpr int kFlagBatch = 3;
+template <int BATCH, typename KeyOf>
 __device__ __forceinline__ bool cells_foreign(const PrepareParams& p, const JobDev& J,
-                                              const CellCoord& cc, int c0, uint32_t win, int shift) {
+                                              const KeyOf& key_of, int c0, uint32_t win,
+                                              int shift) {
   const uint32_t mask = J.cell_cap - 1;
   const CellSlot* base = p.cells + J.cell_off;
-  ulonglong2 v[kFlagBatch];
-  uint32_t h[kFlagBatch];
+  ulonglong2 v[BATCH];
+  uint32_t h[BATCH];
 #pragma unroll
-  for (int t = 0; t < kFlagBatch; ++t) {
-    const int c = c0 + t;
-    h[t] = slot_hash(cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1), mask);
+  for (int t = 0; t < BATCH; ++t) {
+    h[t] = slot_hash(key_of(c0 + t), mask);
     v[t] = __ldg(reinterpret_cast<const ulonglong2*>(base + h[t]));
   }
   bool foreign = false;
 #pragma unroll
-  for (int t = 0; t < kFlagBatch; ++t) {
-    const int c = c0 + t;
-    const uint64_t key = cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1);
+  for (int t = 0; t < BATCH; ++t) {
+    const uint64_t key = key_of(c0 + t);
     if (v[t].x == key) {
       foreign |= slot_foreign(v[t], win, shift);
     } else if (v[t].x != kEmptyKey) {
@@ -473,7 +506,8 @@ __global__ void __launch_bounds__(kWarpTile) k_prep_pad(PrepareParams p) {
 }
 
 // Boundary flags of the kept deposits of flagged jobs: a deposit is a boundary deposit when one of
-// the 27 cells around it holds a deposit of another window. A sphere whose hits in a window are
+// the flag cells around it (27 of side d, or eight of side 2d chosen by cell_nbr) holds a
+// deposit of another window. A sphere whose hits in a window are
 // all non-boundary has no hit in any other window (its hits are within distance d of each other),
 // so the fused kernel can bin it as soon as the window is done.
 // Eight blocks per SM (32 registers): the cell probes are L2 latency, which more warps hide.
@@ -483,7 +517,7 @@ __global__ void __launch_bounds__(kPrepThreads, 8) k_prep_flag(PrepareParams p) 
   const JobDev J = p.jobs[j];
   const JobAux A = p.aux[j];
   if (!A.windowed) return;
-  const int shift = coarse_windows(A) ? 1 : 0;
+  const int shift = coarse_windows(J, A) ? 1 : 0;
   const int64_t k0 = p.blk_offset[b];
   const int cnt = p.blk_count[b];
   for (int q = threadIdx.x; q < cnt; q += kPrepThreads) {
@@ -501,10 +535,18 @@ __global__ void __launch_bounds__(kPrepThreads, 8) k_prep_flag(PrepareParams p) 
     }
     const double z = p.PZ[dst];
     const uint32_t win = (uint32_t)(k / kWindow);
-    const CellCoord cc = cell_of(x, y, z, J.cell_size);
     bool boundary = false;
-    for (int c0 = 0; c0 < 27 && !boundary; c0 += kFlagBatch)
-      boundary = cells_foreign(p, J, cc, c0, win, shift);
+    if (J.cell_nbr8) {
+      const CellNbr nb = cell_nbr(x, y, z, J.cell_size);
+      const auto key_of = [&](int c) { return nbr_key8(nb, c); };
+      for (int c0 = 0; c0 < 8 && !boundary; c0 += 2)
+        boundary = cells_foreign<2>(p, J, key_of, c0, win, shift);
+    } else {
+      const CellCoord cc = cell_of(x, y, z, J.cell_size);
+      const auto key_of = [&](int c) { return nbr_key27(cc, c); };
+      for (int c0 = 0; c0 < 27 && !boundary; c0 += 3)
+        boundary = cells_foreign<3>(p, J, key_of, c0, win, shift);
+    }
     if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
 }
@@ -1280,7 +1322,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_fused(FusedParams P) {
     FusedJob F;
     F.J = P.jobs[W.job];
     F.J.flagged = A.windowed;  // window flags were computed only for these jobs
-    F.win_tiles = coarse_windows(A) ? kCoarseTiles : kWinTiles;
+    F.win_tiles = coarse_windows(F.J, A) ? kCoarseTiles : kWinTiles;
     F.E0 = choose_grid_exponent(A.e_min, A.e_max, F.J.n, A.flags & kAuxNonzero);
     F.n_wt = (A.kept + kWarpTile - 1) / kWarpTile;
     const HistDev H = P.hists[F.J.hist];

@@ -82,7 +82,8 @@ def test_autotune_keeps_state_and_results(work):
                                         ("max_helpers", 8), ("share_divisor", 0),
                                         ("table_slots", 4096), ("flag_min_kept", 0),
                                         ("flag_min_kept", 1 << 40), ("sort_deposits", 0),
-                                        ("sort_deposits", 2)])
+                                        ("sort_deposits", 2), ("flag_cells_limit", 0),
+                                        ("flag_cells_limit", 1 << 50)])
 def test_planning_parameters_do_not_change_results(work, name, value):
     res = []
     for set_it in (False, True):
