@@ -577,13 +577,10 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
   return ST_OK;
 }
 
-// Enqueues jobs [first, last) of the context: uploads, prepare and plan launches, the fused
-// launch, and the copy of the job counters and error flags into pinned host buffers. Nothing
-// waits; finish_range picks the results up.
-// Enqueues the device side of a run on the context's stream: the upload of the job counters,
-// the resets, prepare, plan and fused kernels, and the copies of counters and flags into pinned
-// host memory, with the run's events. While the stream is being captured into a CUDA graph the
-// events become event-record nodes.
+// Enqueues the device side of a run on the context's stream: the resets, the prepare, plan and
+// fused kernels, and the copies of the job counters and error flags into pinned host memory,
+// with the run's events. Nothing waits; finish_range picks the results up. While the stream is
+// being captured into a CUDA graph the events become event-record nodes.
 st_status enqueue_run(st_ctx* c, const st::FusedParams& fp, size_t nj, bool want_export,
                       bool capturing) {
   const unsigned evf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
