@@ -366,6 +366,7 @@ st_status build_tables(st_ctx* c, size_t first, size_t last, bool want_export) {
     D.cell_size = (D.cell_nbr8 ? 2.0 : 1.0) *
                   (J.g.sphereDiameter * (1.0 + 0x1p-10) +
                    (f32 ? J.g.scoringRegionHalfLength * 0x1p-16 : 0.0));
+    D.inv_cell = 1.0 / D.cell_size;
     D.f_HL = (float)J.g.scoringRegionHalfLength;
     D.f_gSO = (float)J.g.greatestSphereOffset;
     D.f_d = (float)J.g.sphereDiameter;

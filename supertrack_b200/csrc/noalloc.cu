@@ -201,6 +201,7 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   const double per_d = (double)n * g.sphereDiameter / (2.0 * g.scoringRegionHalfLength);
   D.cell_nbr8 = (D.flagged && per_d * desc->n_oversamples <= (double)st::kFlagCellsLimit) ? 1 : 0;
   D.cell_size = (D.cell_nbr8 ? 2.0 : 1.0) * g.sphereDiameter * (1.0 + 0x1p-10);
+  D.inv_cell = 1.0 / D.cell_size;
 
   st::JobAux A;
   std::memset(&A, 0, sizeof(A));

@@ -59,6 +59,7 @@ struct JobDev {
   uint32_t cell_cap;
   int64_t cell_off;
   double cell_size;
+  double inv_cell;    // RN(1 / cell_size)
   // FP32 geometry variant: HL', gSO, d, RN(1/d) and r^2 rounded to float (1/d in float)
   float f_HL;
   float f_gSO;

@@ -43,6 +43,13 @@ constexpr double kMagic = 0x1.8p52;             // adding it rounds |q| < 2^51 t
 constexpr double kRiskBand = 0.5 - 0x1p-20;     // |q - rint(q)| at or above it: decide exactly
 constexpr int kGeoBlock = 2;                     // deposits per straight-line geometry block
 
+// The same, for one value: k = llrint(a / d) for |a / d| < 2^21.
+__device__ __forceinline__ double lattice_index(double a, double d, double inv_d) {
+  const double q = st_dmul(a, inv_d);
+  const double k = st_dsub(st_dadd(q, kMagic), kMagic);
+  return fabs(st_dsub(q, k)) >= kRiskBand ? rint(__ddiv_rn(a, d)) : k;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Prepare stage (once per track): four launches.
 //   k_prep_count : per block of kPrepSlotsPerBlock source deposits, the number of deposits that
@@ -95,22 +102,23 @@ __device__ __forceinline__ bool keep_deposit(const JobDev& J, double x, double y
 }
 
 // Flag cell of side cell_size containing (x, y, z): integer cell coordinates, offset to be
-// non-negative. A job's flag cells have a side slightly above d or slightly above 2d
-// (JobDev::cell_nbr8). With side d, two deposits within distance d of each other lie in the same
-// or in adjacent cells: 27 cells around a point hold every deposit within d of it. With side 2d,
-// a deposit within d of a point lies in the point's cell or in the neighbour cell on the side of
-// the half of the cell the point is in: per axis, with u the point's coordinate over the side,
-// |u' - u| < 1/2 - 2^-12 for the other deposit's u', so floor(u') is floor(u) - 1 or floor(u)
-// when u - floor(u) < 1/2, and floor(u) or floor(u) + 1 otherwise (the quotients' rounding
-// errors are far below the margin): eight cells hold every deposit within d.
+// non-negative, from u = RN(c * RN(1/cell_size)) per axis (within |u| 2^-51 of the exact
+// quotient, below 2^-31 for the coordinates of a flagged job, |u| < 2^20). A job's flag cells
+// have a side slightly above d or slightly above 2d (JobDev::cell_nbr8). With side d, two
+// deposits within distance d of each other lie in the same or in adjacent cells: 27 cells around
+// a point hold every deposit within d of it. With side 2d, a deposit within d of a point lies in
+// the point's cell or in the neighbour cell on the side of the half of the cell the point is in:
+// per axis, |u' - u| < 1/2 - 2^-12 for the other deposit's u', so floor(u') is floor(u) - 1 or
+// floor(u) when u - floor(u) < 1/2, and floor(u) or floor(u) + 1 otherwise (the rounding errors
+// are far below the margin): eight cells hold every deposit within d.
 struct CellCoord {
   long long x, y, z;
 };
 
-__device__ __forceinline__ CellCoord cell_of(double x, double y, double z, double cs) {
+__device__ __forceinline__ CellCoord cell_of(double x, double y, double z, double inv_cs) {
   const long long off = 1ll << (kCellBits - 1);
-  return {(long long)floor(__ddiv_rn(x, cs)) + off, (long long)floor(__ddiv_rn(y, cs)) + off,
-          (long long)floor(__ddiv_rn(z, cs)) + off};
+  return {(long long)floor(st_dmul(x, inv_cs)) + off, (long long)floor(st_dmul(y, inv_cs)) + off,
+          (long long)floor(st_dmul(z, inv_cs)) + off};
 }
 
 // The cell of a point (as cell_of) and, per axis, the side of its neighbour cells (-1: the point
@@ -124,9 +132,9 @@ __device__ __forceinline__ int half_side(double u) {
   return st_dsub(u, floor(u)) < 0.5 ? -1 : 1;
 }
 
-__device__ __forceinline__ CellNbr cell_nbr(double x, double y, double z, double cs) {
+__device__ __forceinline__ CellNbr cell_nbr(double x, double y, double z, double inv_cs) {
   const long long off = 1ll << (kCellBits - 1);
-  const double u = __ddiv_rn(x, cs), v = __ddiv_rn(y, cs), w = __ddiv_rn(z, cs);
+  const double u = st_dmul(x, inv_cs), v = st_dmul(y, inv_cs), w = st_dmul(z, inv_cs);
   return {{(long long)floor(u) + off, (long long)floor(v) + off, (long long)floor(w) + off},
           half_side(u), half_side(v), half_side(w)};
 }
@@ -450,7 +458,7 @@ __global__ void __launch_bounds__(kPrepThreads, 4) k_prep_write(PrepareParams p)
       const int64_t k = sorted ? p.blk_offset[b] + s_group[slot_of[r] >> 16] + (slot_of[r] & 0xFFFFu)
                                : run + before + __popc(m[r] & ((1u << lane) - 1u));
       const double az = st_dsub(z1[r], J.gSO);
-      const double kd = rint(__ddiv_rn(az, J.d));
+      const double kd = lattice_index(az, J.d, J.inv_d);
       const double dz = st_dsub(st_dmul(kd, J.d), az);
       const int64_t dst = prep_slot(J, k);
       if (p.fp32) {
@@ -466,7 +474,7 @@ __global__ void __launch_bounds__(kPrepThreads, 4) k_prep_write(PrepareParams p)
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (A.windowed) {
         p.PZ[dst] = z1[r];
-        created_cells += cell_insert(p, J, cell_key(cell_of(x[r], y[r], z1[r], J.cell_size), 0, 0, 0),
+        created_cells += cell_insert(p, J, cell_key(cell_of(x[r], y[r], z1[r], J.inv_cell), 0, 0, 0),
                                      (uint32_t)(k / kWindow));
       }
     }
@@ -537,12 +545,12 @@ __global__ void __launch_bounds__(kPrepThreads, 8) k_prep_flag(PrepareParams p) 
     const uint32_t win = (uint32_t)(k / kWindow);
     bool boundary = false;
     if (J.cell_nbr8) {
-      const CellNbr nb = cell_nbr(x, y, z, J.cell_size);
+      const CellNbr nb = cell_nbr(x, y, z, J.inv_cell);
       const auto key_of = [&](int c) { return nbr_key8(nb, c); };
       for (int c0 = 0; c0 < 8 && !boundary; c0 += 2)
         boundary = cells_foreign<2>(p, J, key_of, c0, win, shift);
     } else {
-      const CellCoord cc = cell_of(x, y, z, J.cell_size);
+      const CellCoord cc = cell_of(x, y, z, J.inv_cell);
       const auto key_of = [&](int c) { return nbr_key27(cc, c); };
       for (int c0 = 0; c0 < 27 && !boundary; c0 += 3)
         boundary = cells_foreign<3>(p, J, key_of, c0, win, shift);

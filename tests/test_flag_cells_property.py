@@ -1,12 +1,12 @@
 """The boundary-flag cell neighbourhoods, restated in float64 (CPU only).
 
 k_prep_flag (supertrack_b200/csrc/vcs_kernels.cu, cell_of / cell_nbr) puts a deposit in the flag
-cell floor(RN(c / s)) per axis, for a side s slightly above d (27 neighbour cells probed) or
+cell floor(RN(c * RN(1/s))) per axis, for a side s slightly above d (27 neighbour cells probed) or
 slightly above 2d (8 probed: per axis the deposit's cell and the neighbour on the side of the half
 of the cell it lies in, u - floor(u) < 1/2 choosing the lower one). A deposit within distance d
 of another must lie in one of the probed cells of the other, or the flag of a sphere with hits in
-two windows could be missed. numpy float64 division and subtraction round like the kernel's
-__ddiv_rn and st_dsub.
+two windows could be missed. numpy float64 products and subtractions round like the kernel's
+st_dmul and st_dsub.
 """
 import numpy as np
 
@@ -15,16 +15,20 @@ def _sides(d):
     return d * (1.0 + 2.0 ** -10), 2.0 * d * (1.0 + 2.0 ** -10)
 
 
+def _cell_u(c, s):
+    return c * (1.0 / s)
+
+
 def _probed27(p, q, s):
-    cp, cq = np.floor(p / s), np.floor(q / s)
+    cp, cq = np.floor(_cell_u(p, s)), np.floor(_cell_u(q, s))
     return np.all(np.abs(cq - cp) <= 1, axis=-1)
 
 
 def _probed8(p, q, s):
-    u = p / s
+    u = _cell_u(p, s)
     cp = np.floor(u)
     side = np.where(u - cp < 0.5, -1.0, 1.0)
-    cq = np.floor(q / s)
+    cq = np.floor(_cell_u(q, s))
     return np.all((cq == cp) | (cq == cp + side), axis=-1)
 
 
@@ -40,7 +44,7 @@ def _pairs(rs, d, n, scale):
     m = n // 4
     frac = rs.choice([0.5, np.nextafter(0.5, 0), np.nextafter(0.5, 1), 0.0, 1e-12,
                       1.0 - 1e-12, 0.25], size=(m, 3))
-    p[-m:] = (np.floor(p[-m:] / s2) + frac) * s2
+    p[-m:] = (np.floor(_cell_u(p[-m:], s2)) + frac) * s2
     q[-m:] = p[-m:]
     axis = rs.integers(0, 3, m)
     q[np.arange(n - m, n), axis] += rs.choice([-d, d], m)
