@@ -176,14 +176,28 @@ __device__ __forceinline__ bool slot_foreign(const ulonglong2& v, uint32_t win, 
          (~(uint32_t)(v.y >> 32) >> shift) != (win >> shift);
 }
 
-// Key of neighbour cell c (0..26) of the 27 around a side-d cell, or (0..7) of the eight around
-// a point in a side-2d cell: offset n.sx on x when bit 0 of c is set, n.sy on y for bit 1, n.sz
-// on z for bit 2.
-__device__ __forceinline__ uint64_t nbr_key27(const CellCoord& cc, int c) {
-  return cell_key(cc, c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1);
+// Neighbour keys as offsets from a cell's key: the coordinate fields of every cell a flagged job
+// probes stay inside [0, 2^kCellBits), so a key of the cell at (dx, dy, dz) from c is c's key plus
+// dz 2^(2 kCellBits) + dy 2^kCellBits + dx in two's complement. Neighbour c (0..26) of the 27
+// around a side-d cell has (c % 3 - 1, c / 3 % 3 - 1, c / 9 - 1); neighbour c (0..7) of the eight
+// around a point in a side-2d cell adds n.sx on x when bit 0 of c is set, n.sy on y for bit 1 and
+// n.sz on z for bit 2.
+__host__ __device__ constexpr int64_t cell_offset(int dx, int dy, int dz) {
+  return (int64_t)dz * ((int64_t)1 << (2 * kCellBits)) + (int64_t)dy * ((int64_t)1 << kCellBits) + dx;
 }
-__device__ __forceinline__ uint64_t nbr_key8(const CellNbr& n, int c) {
-  return cell_key(n.c, (c & 1) ? n.sx : 0, (c & 2) ? n.sy : 0, (c & 4) ? n.sz : 0);
+__device__ __forceinline__ uint64_t nbr_key27(uint64_t base, int c) {
+  return base + (uint64_t)cell_offset(c % 3 - 1, (c / 3) % 3 - 1, c / 9 - 1);
+}
+struct NbrOffsets {
+  uint64_t base;
+  int64_t ox, oy, oz;
+};
+__device__ __forceinline__ NbrOffsets nbr_offsets8(const CellNbr& n) {
+  return {cell_key(n.c, 0, 0, 0), cell_offset(n.sx, 0, 0), cell_offset(0, n.sy, 0),
+          cell_offset(0, 0, n.sz)};
+}
+__device__ __forceinline__ uint64_t nbr_key8(const NbrOffsets& o, int c) {
+  return o.base + (uint64_t)(((c & 1) ? o.ox : 0) + ((c & 2) ? o.oy : 0) + ((c & 4) ? o.oz : 0));
 }
 
 // True when one of the neighbour cells c0 .. c0 + BATCH - 1 (keys from key_of) holds a deposit
@@ -544,16 +558,19 @@ __global__ void __launch_bounds__(kPrepThreads, 8) k_prep_flag(PrepareParams p) 
     const double z = p.PZ[dst];
     const uint32_t win = (uint32_t)(k / kWindow);
     bool boundary = false;
+    // batches unrolled, so that the neighbour offsets are constants
     if (J.cell_nbr8) {
-      const CellNbr nb = cell_nbr(x, y, z, J.inv_cell);
-      const auto key_of = [&](int c) { return nbr_key8(nb, c); };
-      for (int c0 = 0; c0 < 8 && !boundary; c0 += 2)
-        boundary = cells_foreign<2>(p, J, key_of, c0, win, shift);
+      const NbrOffsets o = nbr_offsets8(cell_nbr(x, y, z, J.inv_cell));
+      const auto key_of = [&](int c) { return nbr_key8(o, c); };
+#pragma unroll
+      for (int c0 = 0; c0 < 8; c0 += 2)
+        if (!boundary) boundary = cells_foreign<2>(p, J, key_of, c0, win, shift);
     } else {
-      const CellCoord cc = cell_of(x, y, z, J.inv_cell);
-      const auto key_of = [&](int c) { return nbr_key27(cc, c); };
-      for (int c0 = 0; c0 < 27 && !boundary; c0 += 3)
-        boundary = cells_foreign<3>(p, J, key_of, c0, win, shift);
+      const uint64_t base = cell_key(cell_of(x, y, z, J.inv_cell), 0, 0, 0);
+      const auto key_of = [&](int c) { return nbr_key27(base, c); };
+#pragma unroll
+      for (int c0 = 0; c0 < 27; c0 += 3)
+        if (!boundary) boundary = cells_foreign<3>(p, J, key_of, c0, win, shift);
     }
     if (boundary) p.PKEY[dst] |= kBoundaryBit;
   }
