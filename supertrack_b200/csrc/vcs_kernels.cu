@@ -466,6 +466,8 @@ __global__ void __launch_bounds__(kPrepThreads, 4) k_prep_write(PrepareParams p)
       before += (w < warp) ? c : 0;
       total += c;
     }
+    uint64_t ckey = kEmptyKey;  // windowed jobs: the kept deposit's flag cell and window
+    uint32_t cwin = 0;
     if (keep & (1u << r)) {
       // kept index: block order, or the position of the deposit's group and rank in sorted
       // blocks
@@ -488,9 +490,18 @@ __global__ void __launch_bounds__(kPrepThreads, 4) k_prep_write(PrepareParams p)
       p.PKEY[dst] = (uint64_t)(long long)kd * J.N2;
       if (A.windowed) {
         p.PZ[dst] = z1[r];
-        created_cells += cell_insert(p, J, cell_key(cell_of(x[r], y[r], z1[r], J.inv_cell), 0, 0, 0),
-                                     (uint32_t)(k / kWindow));
+        ckey = cell_key(cell_of(x[r], y[r], z1[r], J.inv_cell), 0, 0, 0);
+        cwin = (uint32_t)(k / kWindow);
       }
+    }
+    if (A.windowed) {
+      // adjacent lanes hold adjacent source deposits, which on dense tracks share a cell and a
+      // window: an insert equal to the previous lane's changes nothing and is skipped, which
+      // spares the cell's slot most of its same-address atomics
+      const uint64_t pkey = __shfl_up_sync(0xffffffffu, ckey, 1);
+      const uint32_t pwin = __shfl_up_sync(0xffffffffu, cwin, 1);
+      if (ckey != kEmptyKey && !(lane > 0 && pkey == ckey && pwin == cwin))
+        created_cells += cell_insert(p, J, ckey, cwin);
     }
     run += total;
   }
