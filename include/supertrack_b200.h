@@ -55,9 +55,9 @@ typedef struct {
 } st_geometry;
 
 /* One track: float64 SoA deposits (x, y, z in nm; edep in eV). on_device != 0 means the four
- * pointers are device addresses that stay valid and unchanged until st_jobs_clear; otherwise
- * they are host memory (pinned memory makes the copy asynchronous) read during st_run. The
- * track is never modified. */
+ * pointers are 8-byte-aligned device addresses (submit rejects others) that stay valid and
+ * unchanged until st_jobs_clear; otherwise they are host memory (pinned memory makes the copy
+ * asynchronous) read during st_run. The track is never modified. */
 typedef struct {
   const double* x;
   const double* y;

@@ -1353,6 +1353,10 @@ st_status st_job_submit(st_ctx* c, const st_track_view* track, const st_job_desc
   if (!c || !track || !desc) return ST_ERR_INVALID_ARGUMENT;
   if (track->n < 0 || (track->n > 0 && (!track->x || !track->y || !track->z || !track->edep)))
     return ST_ERR_INVALID_ARGUMENT;
+  // device arrays are read in place as doubles: a misaligned one would fault the prepare kernels
+  if (track->on_device && track->n > 0 &&
+      (((uintptr_t)track->x | (uintptr_t)track->y | (uintptr_t)track->z | (uintptr_t)track->edep) & 7))
+    return ST_ERR_INVALID_ARGUMENT;
   if (track->n > (int64_t)1 << 40) return ST_ERR_CAPACITY;
   if (desc->hist_id < 0 || desc->hist_id >= (int32_t)c->hists.size()) return ST_ERR_INVALID_ARGUMENT;
   if (desc->zshift < ST_ZSHIFT_PLUS || desc->zshift > ST_ZSHIFT_NONE) return ST_ERR_INVALID_ARGUMENT;

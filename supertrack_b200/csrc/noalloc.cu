@@ -143,6 +143,9 @@ extern "C" st_status st_superimpose_noalloc(const st_track_view* track, const st
   // ---- argument checks (sizes beyond the scratch limits are rejected here)
   if (!track || !desc || !d_counts || !d_yfy) return ST_ERR_INVALID_ARGUMENT;
   if (!track->on_device) return ST_ERR_INVALID_ARGUMENT;
+  if (track->n > 0 &&
+      (((uintptr_t)track->x | (uintptr_t)track->y | (uintptr_t)track->z | (uintptr_t)track->edep) & 7))
+    return ST_ERR_INVALID_ARGUMENT;  // read in place as doubles: a misaligned array would fault
   if (track->n < 0 || (track->n > 0 && (!track->x || !track->y || !track->z || !track->edep)))
     return ST_ERR_INVALID_ARGUMENT;
   if (track->n > kNaMaxDeposits) return ST_ERR_CAPACITY;
