@@ -188,6 +188,10 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *                      while earlier groups compute; groups hold about this many bytes of
  *                      track data (the first and last about a quarter); 0 = one upload, then
  *                      one launch                                            (default 512 MiB)
+ *   pipeline_max_os    ... only when the host tracks average at most this many oversamples
+ *                      per deposit; a batch above it computes longer than it uploads and is
+ *                      uploaded whole, then run at once (each group's launch tail would cost
+ *                      more than the overlap saves)                          (default 50)
  *   graphs             1 = a rerun of the same jobs replays a CUDA graph of the whole run
  *                      (captured at the first rerun); 0 = enqueue every call (default 1)
  *   spill_budget_bytes device bytes for the spill tables (one per resident CTA, each able to

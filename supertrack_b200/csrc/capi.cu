@@ -168,6 +168,10 @@ struct st_ctx {
   // pipelined runs of host tracks: jobs in groups of about pipeline_bytes of track data; the
   // copy stream uploads group g+1 while the context's stream runs group g
   int64_t pipeline_bytes = (int64_t)1 << 29;
+  // ... only when the host tracks average at most this many oversamples per deposit: past it a
+  // batch computes longer than it uploads, and each group's fused-kernel tail costs more than the
+  // overlap saves
+  int64_t pipeline_max_os = 50;
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> up_ev;
   std::vector<int64_t> cache_blk;    // prepare-block prefix of the batch (host copy)
@@ -740,15 +744,21 @@ st_status launch_range(st_ctx* c, size_t first, size_t last, bool want_export, i
   // groups of host track data (one group when every track is on the device): their uploads
   // run on the copy stream, ahead of the groups' kernels. The first and the last group hold
   // about a quarter of pipeline_bytes (the upload before the first kernels and the kernels after
-  // the last upload are not overlapped), the others about pipeline_bytes.
+  // the last upload are not overlapped), the others about pipeline_bytes. A batch averaging more
+  // than pipeline_max_os oversamples per uploaded deposit is uploaded whole, then run at once.
   std::vector<size_t> groups(1, first);
   {
     int64_t total = 0;
+    double host_units = 0.0;
     for (size_t j = first; j < last; ++j)
-      if (!c->jobs[j].track.on_device) total += 32 * c->jobs[j].track.n;
+      if (!c->jobs[j].track.on_device) {
+        total += 32 * c->jobs[j].track.n;
+        host_units += (double)c->jobs[j].track.n * (double)c->jobs[j].desc.n_oversamples;
+      }
+    const bool upload_bound = host_units <= (double)c->pipeline_max_os * (double)(total / 32);
     const int64_t P = c->pipeline_bytes, q = std::max<int64_t>(P / 4, 1);
     std::vector<int64_t> cuts;
-    if (total > 2 * q) {
+    if (total > 2 * q && upload_bound) {
       for (int64_t t = q; t < total - q && cuts.size() < 62; t += P) cuts.push_back(t);
       cuts.push_back(total - q);
     }
@@ -1124,6 +1134,7 @@ st_status st_ctx_set_param(st_ctx* c, const char* name, int64_t v) {
   else if (n == "spill_budget_bytes" && v >= 0) c->spill_budget = v;
   else if (n == "table_slots" && (v == 0 || v == 4096 || v == 8192)) c->table_slots = (int)v;
   else if (n == "pipeline_bytes" && v >= 0) c->pipeline_bytes = v > 0 ? v : ((int64_t)1 << 62);
+  else if (n == "pipeline_max_os" && v >= 0) c->pipeline_max_os = v;
   else if (n == "graphs" && (v == 0 || v == 1)) { c->use_graphs = v != 0; drop_graph(c); }
   else return ST_ERR_INVALID_ARGUMENT;
   c->cache_valid = false;
@@ -1146,6 +1157,7 @@ st_status st_ctx_get_param(const st_ctx* c, const char* name, int64_t* v) {
   else if (n == "spill_budget_bytes") *v = c->spill_budget;
   else if (n == "table_slots") *v = c->table_slots;
   else if (n == "pipeline_bytes") *v = c->pipeline_bytes;
+  else if (n == "pipeline_max_os") *v = c->pipeline_max_os;
   else if (n == "graphs") *v = c->use_graphs ? 1 : 0;
   else if (n == "graph_launches") *v = c->graph_launches;  // read-only: runs replayed from a graph
   else if (n == "last_grid") *v = c->cache_grid;       // read-only: CTAs of the last fused launch

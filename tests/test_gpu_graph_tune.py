@@ -99,12 +99,14 @@ def test_planning_parameters_do_not_change_results(work, name, value):
 
 def test_pipelined_host_tracks_equal_single_launch(work):
     """Host tracks in several upload groups (copy stream ahead of each group's kernels) give the
-    same spectra and statistics as one upload and one launch."""
+    same spectra and statistics as one upload and one launch; a batch past pipeline_max_os
+    oversamples per deposit is uploaded whole even with small groups asked for."""
     host = [t.cpu().numpy() for t in (work.x, work.y, work.z, work.edep)]
     res = []
-    for pipeline_bytes in (0, 1 << 20):
+    for pipeline_bytes, max_os in ((0, 50), (1 << 20, 1 << 40), (1 << 20, 0)):
         with st.Context(0) as c:
             c.set_param("pipeline_bytes", pipeline_bytes)
+            c.set_param("pipeline_max_os", max_os)
             hs = [c.histogram(*h) for h in work.hists]
             for j in range(work.n_jobs):
                 o, n = int(work.offsets[j]), int(work.sizes[j])
@@ -119,7 +121,9 @@ def test_pipelined_host_tracks_equal_single_launch(work):
                 c.run("batched")
             res.append((_spectra(c, hs), [c.stats(j) for j in range(work.n_jobs)],
                         c.last_timing()[2]))
-    ((c0, y0), s0, l0), ((c1, y1), s1, l1) = res
+    ((c0, y0), s0, l0), ((c1, y1), s1, l1), ((c2, y2), s2, l2) = res
     assert l1 > l0                            # the second form launched kernels per group
+    assert l2 == l0                           # the third uploaded whole: one launch sequence
     assert_hist_equal(c1, y1, c0, y0)
-    assert s0 == s1
+    assert_hist_equal(c2, y2, c0, y0)
+    assert s0 == s1 == s2
