@@ -187,7 +187,7 @@ ST_API st_status st_ctx_set_tuning(st_ctx* ctx, int64_t item_cost, int32_t grid)
  *   pipeline_bytes     runs with host-resident tracks upload them in groups on a second stream
  *                      while earlier groups compute; groups hold about this many bytes of
  *                      track data (the first and last about a quarter); 0 = one upload, then
- *                      one launch                                            (default 512 MiB)
+ *                      one launch                                            (default 256 MiB)
  *   pipeline_max_os    ... only when the host tracks average at most this many oversamples
  *                      per deposit; a batch above it computes longer than it uploads and is
  *                      uploaded whole, then run at once (each group's launch tail would cost

@@ -167,7 +167,7 @@ struct st_ctx {
   int table_slots = 0;        // shared-memory sphere table: 0 automatic, 4096 or 8192
   // pipelined runs of host tracks: jobs in groups of about pipeline_bytes of track data; the
   // copy stream uploads group g+1 while the context's stream runs group g
-  int64_t pipeline_bytes = (int64_t)1 << 29;
+  int64_t pipeline_bytes = (int64_t)1 << 28;
   // ... only when the host tracks average at most this many oversamples per deposit: past it a
   // batch computes longer than it uploads, and each group's fused-kernel tail costs more than the
   // overlap saves
