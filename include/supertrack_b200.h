@@ -147,6 +147,15 @@ ST_API st_status st_ctx_last_timing(const st_ctx* ctx, float* prepare_ms, float*
                                     int32_t* launches);
 /* Measured FP64 add/multiply issue rate of the device (operations per second). */
 ST_API st_status st_measure_fp64_peak(st_ctx* ctx, double* ops_per_second);
+/* Runs, on the context's stream, the fused kernel's one cross-CTA wait (a helper of a shared
+ * unit waiting for the unit's spill table to be published) against a unit table set to
+ * `published` (>= 0), or never published (< 0), with at most max_polls sleeps (at most 2^24,
+ * the fused kernel's own limit). *table receives what the wait got (-1 when it ran out) and
+ * *error_flags the device error flags it set (8: a wait ran out, which st_run reports as
+ * ST_ERR_DEVICE_WAIT). No counterpart in the reference: it checks on the device, without a
+ * fault or a hang, that the wait gives up and reports instead of waiting forever. */
+ST_API st_status st_probe_unit_wait(st_ctx* ctx, int32_t published, int64_t max_polls,
+                                    int32_t* table, int32_t* error_flags);
 /* Measured rate of conflict-free 64-bit shared-memory atomic additions of the device (one CTA
  * of 1024 threads per SM, the fused kernel's shape), in atomics per second. No counterpart in the
  * reference: the peak that the shared-memory roofline term of the fused kernel is set against. */

@@ -344,6 +344,14 @@ class Context:
                     "st_measure_smem_atomic_peak")
         return v.value
 
+    def probe_unit_wait(self, published: int, max_polls: int):
+        """The fused kernel's bounded wait for a shared unit's table, against a table that is
+        published (>= 0) or never is (< 0): returns (table it got, device error flags)."""
+        t, f = C.c_int32(), C.c_int32()
+        self._check(lib().st_probe_unit_wait(self._h, published, max_polls, C.byref(t),
+                                             C.byref(f)), "st_probe_unit_wait")
+        return t.value, f.value
+
     # jobs -----------------------------------------------------------------------------------
     def submit(self, x, y, z, edep, *, half_length: float, sphere_diameter: float,
                n_oversamples: int, hist: int, seed: int = 0, track_id: int = 0,

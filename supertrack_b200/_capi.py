@@ -133,6 +133,8 @@ SIGNATURES = [
     ("st_job_submit_many", C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("st_measure_fp64_peak", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("st_measure_smem_atomic_peak", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("st_probe_unit_wait", C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)]),
     ("st_jobs_count", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     ("st_run_export", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     ("st_run_async", C.c_int, [C.c_void_p]),

@@ -20,6 +20,8 @@ cudaError_t launch_prepare(const PrepareParams& p, int64_t n_blocks, bool any_fl
 cudaError_t configure_fused();
 cudaError_t launch_fused(FusedParams p, int max_nbins, int grid, int table_slots, cudaStream_t s);
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s);
+cudaError_t launch_unit_wait_probe(int* table, int* error_flags, int* out, long long max_polls,
+                                   cudaStream_t s);
 cudaError_t launch_smem_atomic_probe(unsigned long long* out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_plan(const PlanParams& q, cudaStream_t s);
 cudaError_t launch_reset_aux(JobAux* aux, int n, cudaStream_t s);
@@ -1502,6 +1504,32 @@ st_status st_measure_fp64_peak(st_ctx* c, double* ops_per_second) {
   // two FP64 operations (one multiply, one add) per chain step
   *ops_per_second = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (best * 1e-3);
   return ST_OK;
+}
+
+st_status st_probe_unit_wait(st_ctx* c, int32_t published, int64_t max_polls, int32_t* table,
+                             int32_t* error_flags) {
+  if (!c || !table || !error_flags || max_polls < 0 || max_polls > ((int64_t)1 << 24))
+    return ST_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->device);
+  DevBuf buf;
+  ST_CUDA(ensure(buf, 16), "wait probe buffer");
+  // the unit's table slot: published, or "being acquired" (-2) by a first helper that never
+  // publishes it; then the error flags and the probe's result
+  const int init[3] = {published >= 0 ? published : -2, 0, 0};
+  int out[3] = {0, 0, 0};
+  int* d = (int*)buf.p;
+  st_status s = ST_OK;
+  if (cudaMemcpyAsync(d, init, sizeof(init), cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      st::launch_unit_wait_probe(d, d + 1, d + 2, (long long)max_polls, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(out, d, sizeof(out), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    c->err = std::string("wait probe: ") + cudaGetErrorString(cudaGetLastError());
+    s = ST_ERR_CUDA;
+  }
+  release(buf);
+  *table = out[2];
+  *error_flags = out[1];
+  return s;
 }
 
 st_status st_measure_smem_atomic_peak(st_ctx* c, double* atomics_per_second) {

@@ -889,16 +889,18 @@ __device__ __forceinline__ void pool_release(unsigned int* bits, int t) {
   atomicAnd(&bits[t >> 5], ~(1u << (t & 31)));
 }
 
-// Table of shared unit u: the first helper acquires it, the others wait (bounded) until it is
-// published.
-__device__ int unit_table_get(const FusedParams& P, int u) {
+// Table of shared unit u: the first helper acquires it, the others wait (bounded: max_polls
+// sleeps of at least 64 ns) until it is published. A wait that runs out sets error flag 8 and
+// returns -1, and the item is given up; the host reports the run as ST_ERR_DEVICE_WAIT.
+constexpr long long kUnitWaitPolls = 1ll << 24;
+__device__ int unit_table_get(const FusedParams& P, int u, long long max_polls = kUnitWaitPolls) {
   int t = atomicCAS(&P.unit_table[u], -1, -2);
   if (t == -1) {
     t = pool_acquire(P.pool_bits, gridDim.x, P.error_flags);
     atomicExch(&P.unit_table[u], t < 0 ? -3 : t);
     return t;
   }
-  for (long long spin = 0; t == -2 && spin < (1ll << 24); ++spin) {
+  for (long long spin = 0; t == -2 && spin < max_polls; ++spin) {
     __nanosleep(64);
     t = *(volatile int*)&P.unit_table[u];
   }
@@ -1678,6 +1680,21 @@ __global__ void __launch_bounds__(256) k_fp64_probe(double* out, int iters, doub
 #pragma unroll
   for (int k = 0; k < 8; ++k) s += v[k];
   if (s == 12345.678) out[blockIdx.x] = s;  // keeps the chains alive
+}
+
+// One helper's wait for the table of shared unit 0 (unit_table_get), with max_polls sleeps;
+// out[0] receives the table it got (-1: the wait ran out).
+__global__ void k_unit_wait_probe(FusedParams p, long long max_polls, int* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = unit_table_get(p, 0, max_polls);
+}
+
+cudaError_t launch_unit_wait_probe(int* table, int* error_flags, int* out, long long max_polls,
+                                   cudaStream_t s) {
+  FusedParams p{};
+  p.unit_table = table;
+  p.error_flags = error_flags;
+  k_unit_wait_probe<<<1, 32, 0, s>>>(p, max_polls, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fp64_probe(double* out, int blocks, int iters, cudaStream_t s) {
