@@ -614,6 +614,28 @@ def headline(args, rank, world, dev, stream):
         e2e = {"value": units * e2e_steps / (E.ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(nb * 16) * world,
                "steps": e2e_steps}
+        # the upload's roofline (untimed): this rank's track bytes per step over the e2e step
+        # time, against one plain pinned host-to-device copy of its x array on the same link
+        mine_bytes = int(w.sizes[mine].sum()) * 32
+        dst = torch.empty(hx[0].shape, dtype=hx[0].dtype, device=dev)
+        best = None
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                dst.copy_(hx[0], non_blocking=True)
+                b.record(stream)
+                b.synchronize()
+                t = a.elapsed_time(b)
+                best = t if best is None else min(best, t)
+        copy_gbs = hx[0].numel() * 8 / (best * 1e-3) / 1e9
+        achieved = mine_bytes / (E.ms / e2e_steps * 1e-3) / 1e9
+        e2e["pcie"] = {"achieved_gbs": achieved, "copy_gbs": copy_gbs, "frac": achieved / copy_gbs,
+                       "copy": "one pinned cudaMemcpyAsync of this rank's x array "
+                               f"({hx[0].numel() * 8 / 1e9:.2f} GB), best of 3",
+                       "rank_bytes_per_step": mine_bytes}
+        del dst
         ctx2.close()
         del hx
 
